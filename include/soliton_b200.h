@@ -1,0 +1,142 @@
+/*
+ * soliton_b200.h -- C ABI of the B200-native soliton_solver flow backend.
+ *
+ * The library (libsoliton_b200.so) implements, as hand-written sm_100a CUDA
+ * kernels, the per-theory energy-gradient stencils, the arrested-Newton-flow
+ * RK4 step with unit-norm re-projection, and the energy / topological-charge
+ * reductions of soliton_solver, for the Chiral magnet, Baby Skyrme model,
+ * Ginzburg-Landau (Abelian Higgs) and anisotropic s+id superconductor theories.
+ *
+ * Conventions
+ *  - Every function returns an int status (SS_OK == 0).  ss_last_error() gives a
+ *    thread-local message for the last failing call.
+ *  - Parameters are the reference's packed arrays: p_i (int32) and p_f (float64)
+ *    exactly as produced by each theory's pack_device_params
+ *    (soliton_solver/core/params.py:229-249 plus the theory's params.py).
+ *  - Buffers are device pointers owned by the caller.  Fields use the reference
+ *    layout idx = y + x*ylen + a*xlen*ylen (soliton_solver/core/utils.py:17-42)
+ *    in the handle's element type (double for SS_FP64 / SS_PLAIN_FP64, float for
+ *    SS_FP32).  Densities are always double.
+ *  - The library never allocates device memory: the caller provides a workspace
+ *    of ss_workspace_bytes() bytes through ss_bind().
+ *  - Work is issued on the stream given to ss_bind() (a cudaStream_t, NULL for the
+ *    legacy default stream).  Functions that return host scalars synchronise that
+ *    stream; the *_async variants do not.
+ */
+#ifndef SOLITON_B200_H
+#define SOLITON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SS_ABI_VERSION 1
+
+/* status codes */
+#define SS_OK 0
+#define SS_ERR_ARG 1          /* bad argument, unsupported parameter combination */
+#define SS_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define SS_ERR_NONFINITE 3    /* a reduction produced NaN or Inf */
+#define SS_ERR_STATE 4        /* call out of order (e.g. no workspace bound) */
+#define SS_ERR_WORKSPACE 5    /* workspace too small or misaligned */
+
+/* theories (THEORY_SPEC names of the reference theory packages) */
+#define SS_THEORY_CHIRAL_MAGNET 0   /* theories/chiral_magnet */
+#define SS_THEORY_BABY_SKYRME 1     /* theories/baby_skyrme */
+#define SS_THEORY_GINZBURG_LANDAU 2 /* theories/ginzburg_landau_superconductor */
+#define SS_THEORY_ANISOTROPIC 3     /* theories/anisotropic_superconductor (s+id) */
+
+/* precision / method */
+#define SS_FP64 0       /* fused single-pass-per-stage kernels, FP64 fields */
+#define SS_FP32 1       /* fused kernels, FP32 fields, FP64 energy/charge reductions */
+#define SS_PLAIN_FP64 2 /* reference-structured FP64 form: derivative buffers, one
+                           launch per RK stage, host-side arrest */
+
+/* charges */
+#define SS_CHARGE_SKYRMION 0 /* m.(dx m x dy m) dA/4pi : chiral magnet, baby Skyrme */
+#define SS_CHARGE_MAGNETIC 1 /* -div m dA : chiral magnet */
+#define SS_CHARGE_VORTEX 2   /* (dx A2 - dy A1) dA/(2 pi q) : Ginzburg-Landau, s+id */
+
+/* couplings for ss_coupling_grad (partial derivatives of E at fixed field) */
+#define SS_COUPLING_KAPPA 0  /* baby Skyrme kappa */
+#define SS_COUPLING_MPI 1    /* baby Skyrme mpi */
+#define SS_COUPLING_LAMBDA 2 /* Ginzburg-Landau Lambda */
+#define SS_COUPLING_B 3      /* chiral magnet applied field B (through coup_h) */
+#define SS_COUPLING_D 4      /* chiral magnet DMI strength D (through coup_K, coup_h, coup_mu) */
+#define SS_COUPLING_K 5      /* chiral magnet anisotropy K (through coup_K) */
+
+typedef struct ss_handle ss_handle;
+
+int ss_abi_version(void);
+const char *ss_status_string(int status);
+const char *ss_last_error(void);
+
+/* Create a solver handle for one lattice.  Replaces Simulation.__init__'s
+ * parameter resolution and packing (soliton_solver/core/simulation.py:43-115). */
+int ss_create(int theory, const int32_t *p_i, int n_i, const double *p_f, int n_f, int precision,
+              ss_handle **out);
+int ss_destroy(ss_handle *h);
+/* Bytes of caller-owned device workspace ss_bind() needs (l1..l3, the Field/Velocity
+ * ping-pong copies, reduction partials and the device-side step state). */
+int ss_workspace_bytes(const ss_handle *h, size_t *bytes);
+/* Bind the caller's Field and Velocity buffers, the workspace and the stream. */
+int ss_bind(ss_handle *h, void *field, void *velocity, void *workspace, size_t workspace_bytes,
+            void *stream);
+
+/* n_steps arrested-Newton-flow RK4 steps of the bound Field/Velocity.
+ * Replaces Simulation.step / do_arrested_newton_flow
+ * (soliton_solver/core/simulation.py:388-409, core/integrator.py:217-348).
+ * energy_traj[s] / err_traj[s] (host, nullable) receive E after step s and the
+ * signed maximum of the stage-4 energy gradient of step s.  prev_energy is the
+ * energy the first step's arrest test compares against; pass NaN to continue from
+ * the energy the previous ss_step call left on the device. */
+int ss_step(ss_handle *h, int n_steps, double prev_energy, double *energy_traj, double *err_traj);
+/* As ss_step but without a host synchronisation: the trajectories go to device
+ * arrays of n_steps doubles (nullable) and the status of the device-side checks is
+ * reported by the next synchronising call or ss_check_status(). */
+int ss_step_async(ss_handle *h, int n_steps, double prev_energy, double *energy_traj_dev,
+                  double *err_traj_dev);
+/* Synchronise the bound stream and return the status the device-side checks set. */
+int ss_check_status(ss_handle *h);
+
+/* One gradient evaluation of an arbitrary field buffer: energy_gradient (nullable)
+ * receives the theory's projected dE/dphi, l_out (nullable) receives -dt*dE/dphi.
+ * Replaces theory.kernels.do_gradient_step_kernel(l_out, Field, d1, d2, EG, p_i, p_f)
+ * (core/integrator.py:15-48 with e.g. theories/chiral_magnet/kernels.py:398-511). */
+int ss_gradient(ss_handle *h, const void *field, void *energy_gradient, void *l_out);
+/* Per-site energy x dA (double).  Replaces compute_energy_kernel
+ * (e.g. theories/chiral_magnet/kernels.py:219-251). */
+int ss_energy_density(ss_handle *h, const void *field, double *density);
+/* Total energy, fixed-order compensated FP64 sum.  Replaces observables.compute_energy
+ * (e.g. theories/chiral_magnet/observables.py:15-57). */
+int ss_energy(ss_handle *h, const void *field, double *out);
+/* Charge densities / totals.  Replace compute_skyrmion_number_kernel,
+ * compute_magnetic_charge_kernel, compute_vortex_number_kernel and the matching
+ * observables.compute_* (e.g. theories/chiral_magnet/kernels.py:294-395,
+ * theories/ginzburg_landau_superconductor/kernels.py:181-215). */
+int ss_charge_density(ss_handle *h, const void *field, int which, double *density);
+int ss_charge(ss_handle *h, const void *field, int which, double *out);
+/* Partial derivative dE/dc of the discrete energy with respect to a coupling at
+ * fixed field.  At a relaxed (stationary) field this is dE_min/dc by the envelope
+ * theorem.  No reference counterpart: a new capability of this backend. */
+int ss_coupling_grad(ss_handle *h, const void *field, int coupling, double *out);
+
+/* The reference's RK4 building blocks on arbitrary buffers (element type of the
+ * handle).  ss_rk4_stage replaces do_rk4_step_kernel (core/integrator.py:51-96):
+ * k_out = dt*(velocity + factor*l_in), temp = field + factor*k_prev.
+ * ss_rk4_finalize replaces the theory's do_rk4_kernel / do_rk4_kernel_no_constraint
+ * (core/integrator.py:99-189). */
+int ss_rk4_stage(ss_handle *h, void *k_out, const void *velocity, const void *l_in, void *temp,
+                 const void *field, const void *k_prev, double factor);
+int ss_rk4_finalize(ss_handle *h, void *velocity, void *field, const void *k1, const void *k2,
+                    const void *k3, const void *k4, const void *l1, const void *l2, const void *l3,
+                    const void *l4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOLITON_B200_H */

@@ -1,0 +1,200 @@
+"""Python owner of one native solver handle (libsoliton_b200).
+
+``Solver`` creates the handle from the reference's packed ``p_i``/``p_f`` arrays,
+allocates the caller-owned device workspace as a torch tensor and forwards every
+call to the C ABI on the bound CUDA stream.  Device buffers are torch tensors (or
+anything exposing ``data_ptr()``); they must be contiguous, on the solver's
+device and of the solver's element type.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from soliton_solver_b200 import _native as nat
+
+_CHARGES = {"skyrmion": nat.SS_CHARGE_SKYRMION, "magnetic": nat.SS_CHARGE_MAGNETIC, "vortex": nat.SS_CHARGE_VORTEX}
+_COUPLINGS = {"kappa": nat.SS_COUPLING_KAPPA, "mpi": nat.SS_COUPLING_MPI, "Lambda": nat.SS_COUPLING_LAMBDA,
+              "coup_K": nat.SS_COUPLING_COUP_K, "coup_h": nat.SS_COUPLING_COUP_H,
+              "coup_mu": nat.SS_COUPLING_COUP_MU}
+
+
+def _ptr(t) -> int | None:
+    if t is None:
+        return None
+    if isinstance(t, torch.Tensor):
+        return t.data_ptr()
+    cai = getattr(t, "__cuda_array_interface__", None)
+    if cai is not None:
+        return int(cai["data"][0])
+    raise TypeError(f"expected a CUDA tensor, got {type(t)!r}")
+
+
+class Solver:
+    """One lattice of one theory on one CUDA device."""
+
+    def __init__(self, theory_id: int, p_i, p_f, precision: str = "fp32", device=None, stream=None):
+        lib = nat.load()
+        if precision not in nat.PRECISIONS:
+            raise ValueError(f"precision must be one of {tuple(nat.PRECISIONS)}")
+        self.precision = precision
+        self.dtype = torch.float32 if precision == "fp32" else torch.float64
+        self.p_i = np.ascontiguousarray(p_i, dtype=np.int32)
+        self.p_f = np.ascontiguousarray(p_f, dtype=np.float64)
+        self.theory_id = int(theory_id)
+        self.xlen, self.ylen, self.nf = int(self.p_i[0]), int(self.p_i[1]), int(self.p_i[4])
+        self.N = self.xlen * self.ylen
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        h = ctypes.c_void_p()
+        nat.check(lib.ss_create(self.theory_id, self.p_i.ctypes.data, len(self.p_i), self.p_f.ctypes.data,
+                                len(self.p_f), nat.PRECISIONS[precision], ctypes.byref(h)))
+        self._h = h
+        self._lib = lib
+        nbytes = ctypes.c_size_t()
+        nat.check(lib.ss_workspace_bytes(h, ctypes.byref(nbytes)))
+        self.workspace = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+        self.field = None
+        self.velocity = None
+        self.stream = stream
+        self._bind(None, None)
+
+    # ------------------------------------------------------------------ binding
+    def _stream_handle(self):
+        if self.stream is not None:
+            return int(self.stream.cuda_stream) if hasattr(self.stream, "cuda_stream") else int(self.stream)
+        return int(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _bind(self, field, velocity):
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_bind(self._h, _ptr(field), _ptr(velocity), self.workspace.data_ptr(),
+                                        self.workspace.numel(), self._stream_handle()))
+        self.field, self.velocity = field, velocity
+
+    def bind(self, field: torch.Tensor, velocity: torch.Tensor):
+        """Bind the Field/Velocity buffers that ``step`` advances in place."""
+        self._check(field)
+        self._check(velocity)
+        self._bind(field, velocity)
+
+    def _check(self, t, dtype=None):
+        if not isinstance(t, torch.Tensor):
+            return
+        want = dtype or self.dtype
+        if t.dtype != want or t.device != self.device or not t.is_contiguous():
+            raise ValueError(f"buffer must be a contiguous {want} tensor on {self.device}")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and getattr(self, "_lib", None) is not None:
+            try:
+                self._lib.ss_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # ------------------------------------------------------------------ flow
+    def step(self, n_steps: int = 1, prev_energy: float = math.nan):
+        """Advance the bound buffers; returns (energy_traj, err_traj) numpy arrays."""
+        E = np.empty(max(n_steps, 0))
+        err = np.empty(max(n_steps, 0))
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_step(self._h, int(n_steps), float(prev_energy), E.ctypes.data, err.ctypes.data))
+        return E, err
+
+    def step_async(self, n_steps: int, prev_energy: float = math.nan, energy_traj=None, err_traj=None):
+        """Advance without a host synchronisation; trajectories go to device tensors."""
+        for t in (energy_traj, err_traj):
+            if t is not None:
+                self._check(t, torch.float64)
+                if t.numel() < n_steps:
+                    raise ValueError("trajectory buffer shorter than n_steps")
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_step_async(self._h, int(n_steps), float(prev_energy), _ptr(energy_traj),
+                                              _ptr(err_traj)))
+
+    def check_status(self):
+        nat.check(self._lib.ss_check_status(self._h))
+
+    # ------------------------------------------------------------------ hooks
+    def gradient(self, field, energy_gradient=None, l_out=None):
+        for t in (field, energy_gradient, l_out):
+            if t is not None:
+                self._check(t)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_gradient(self._h, _ptr(field), _ptr(energy_gradient), _ptr(l_out)))
+
+    def energy(self, field) -> float:
+        self._check(field)
+        out = ctypes.c_double()
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_energy(self._h, _ptr(field), ctypes.byref(out)))
+        return out.value
+
+    def energy_density(self, field, out=None):
+        self._check(field)
+        out = out if out is not None else torch.empty(self.N, dtype=torch.float64, device=self.device)
+        self._check(out, torch.float64)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_energy_density(self._h, _ptr(field), _ptr(out)))
+        return out
+
+    def charge(self, field, which: str) -> float:
+        self._check(field)
+        out = ctypes.c_double()
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_charge(self._h, _ptr(field), _CHARGES[which], ctypes.byref(out)))
+        return out.value
+
+    def charge_density(self, field, which: str, out=None):
+        self._check(field)
+        out = out if out is not None else torch.empty(self.N, dtype=torch.float64, device=self.device)
+        self._check(out, torch.float64)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_charge_density(self._h, _ptr(field), _CHARGES[which], _ptr(out)))
+        return out
+
+    def coupling_grad(self, field, which: str) -> float:
+        self._check(field)
+        out = ctypes.c_double()
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_coupling_grad(self._h, _ptr(field), _COUPLINGS[which], ctypes.byref(out)))
+        return out.value
+
+    def rk4_stage(self, k_out, velocity, l_in, temp, field, k_prev, factor: float):
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_rk4_stage(self._h, _ptr(k_out), _ptr(velocity), _ptr(l_in), _ptr(temp),
+                                             _ptr(field), _ptr(k_prev), float(factor)))
+
+    def rk4_finalize(self, velocity, field, k1, k2, k3, k4, l1, l2, l3, l4):
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_rk4_finalize(self._h, _ptr(velocity), _ptr(field), *(
+                _ptr(t) for t in (k1, k2, k3, k4, l1, l2, l3, l4))))
+
+
+_CACHE: dict = {}
+
+
+def solver_for(theory_id: int, p_i, p_f, dtype, device) -> Solver:
+    """Cached solver for hook-style calls that pass packed parameter arrays."""
+    p_i = np.ascontiguousarray(_to_host(p_i), dtype=np.int32)
+    p_f = np.ascontiguousarray(_to_host(p_f), dtype=np.float64)
+    precision = "fp32" if dtype == torch.float32 else "fp64"
+    key = (theory_id, precision, str(device), p_i.tobytes(), p_f.tobytes())
+    s = _CACHE.get(key)
+    if s is None:
+        if len(_CACHE) > 64:
+            _CACHE.clear()
+        s = Solver(theory_id, p_i, p_f, precision, device)
+        _CACHE[key] = s
+    return s
+
+
+def _to_host(a):
+    if isinstance(a, torch.Tensor):
+        return a.detach().cpu().numpy()
+    if hasattr(a, "copy_to_host"):
+        return a.copy_to_host()
+    return np.asarray(a)

@@ -1,0 +1,759 @@
+// abi.cu -- C ABI of libsoliton_b200 (declared in include/soliton_b200.h).
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/soliton_b200.h"
+#include "common.cuh"
+#include "flow.cuh"
+#include "plain.cuh"
+#include "theories.cuh"
+
+using namespace ssb;
+
+namespace {
+
+constexpr int TX = 16, TY = 64, NT = 256;  // fused tile: 16 x 64 sites, 256 threads
+constexpr int TRAJ_CAP = 1024;              // device trajectory slots used by ss_step
+constexpr size_t ALIGN = 256;
+
+thread_local char g_err[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) return fail(SS_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+size_t align_up(size_t v) { return (v + ALIGN - 1) / ALIGN * ALIGN; }
+
+}  // namespace
+
+struct ss_handle {
+  int theory = 0, precision = 0, nf = 0;
+  Grid G{};
+  Phys P{};
+  size_t elem = 8;
+  int nblocks = 0;        // fused tiles
+  int plain_sum_blocks = 0, plain_max_blocks = 0;
+  // bound buffers
+  void* field = nullptr;
+  void* vel = nullptr;
+  char* ws = nullptr;
+  size_t ws_bytes = 0;
+  cudaStream_t stream = nullptr;
+  // workspace carve (fused)
+  StepState* st = nullptr;
+  double* partial = nullptr;
+  double* traj_E = nullptr;
+  double* traj_err = nullptr;
+  void* l[4] = {nullptr, nullptr, nullptr, nullptr};
+  void* phi_alt = nullptr;
+  void* vel_alt = nullptr;
+  // plain extras
+  void* k[4] = {nullptr, nullptr, nullptr, nullptr};
+  void* temp = nullptr;
+  void* eg = nullptr;
+  double* d1 = nullptr;
+  double* d2 = nullptr;
+  double* en = nullptr;
+  double* entmp = nullptr;
+  double E_last_host = NAN;
+  std::vector<double> host_partial;
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// workspace layout
+// ---------------------------------------------------------------------------
+size_t layout(ss_handle* h, char* base) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> char* {
+    char* p = base ? base + off : nullptr;
+    off = align_up(off + bytes);
+    return p;
+  };
+  const size_t field_bytes = h->elem * (size_t)h->nf * (size_t)h->G.N;
+  h->st = (StepState*)take(sizeof(StepState));
+  const size_t np = (size_t)std::max(h->nblocks, std::max(h->plain_sum_blocks, h->plain_max_blocks));
+  h->partial = (double*)take(np * sizeof(double));
+  h->traj_E = (double*)take(TRAJ_CAP * sizeof(double));
+  h->traj_err = (double*)take(TRAJ_CAP * sizeof(double));
+  if (h->precision == SS_PLAIN_FP64) {
+    for (int i = 0; i < 4; ++i) h->k[i] = take(field_bytes);
+    for (int i = 0; i < 4; ++i) h->l[i] = take(field_bytes);
+    h->temp = take(field_bytes);
+    h->eg = take(field_bytes);
+    h->d1 = (double*)take(2 * field_bytes);
+    h->d2 = (double*)take(4 * field_bytes);
+    h->en = (double*)take((size_t)h->G.N * sizeof(double));
+    h->entmp = (double*)take((size_t)h->G.N * sizeof(double));
+  } else {
+    for (int i = 0; i < 3; ++i) h->l[i] = take(field_bytes);
+    h->l[3] = nullptr;
+    h->phi_alt = take(field_bytes);
+    h->vel_alt = take(field_bytes);
+  }
+  return off;
+}
+
+// ---------------------------------------------------------------------------
+// parameter decoding (packed arrays of each theory's pack_device_params)
+// ---------------------------------------------------------------------------
+int decode(ss_handle* h, int theory, const int32_t* p_i, int n_i, const double* p_f, int n_f) {
+  static const int need_i[4] = {16, 20, 12, 14};
+  static const int need_f[4] = {15, 14, 11, 25};
+  static const int theory_nf[4] = {4, 3, 4, 6};
+  if (theory < 0 || theory > 3) return fail(SS_ERR_ARG, "unknown theory id %d", theory);
+  if (!p_i || !p_f) return fail(SS_ERR_ARG, "p_i/p_f must not be NULL");
+  if (n_i < need_i[theory] || n_f < need_f[theory])
+    return fail(SS_ERR_ARG, "packed params too short for theory %d: n_i=%d (need %d), n_f=%d (need %d)", theory, n_i,
+                need_i[theory], n_f, need_f[theory]);
+  Grid& G = h->G;
+  G.X = p_i[0];
+  G.Y = p_i[1];
+  G.halo = p_i[2];
+  const int nc = p_i[3], nf = p_i[4];
+  if (G.X < 1 || G.Y < 1) return fail(SS_ERR_ARG, "xlen/ylen must be positive (got %d, %d)", G.X, G.Y);
+  if (nc != 2) return fail(SS_ERR_ARG, "number_coordinates must be 2 (got %d)", nc);
+  if (nf != theory_nf[theory])
+    return fail(SS_ERR_ARG, "number_total_fields=%d but theory %d has %d components", nf, theory, theory_nf[theory]);
+  if (G.halo < 2) return fail(SS_ERR_ARG, "halo must be >= 2 for the 5-point stencils (got %d)", G.halo);
+  G.N = (long long)G.X * G.Y;
+  if ((long long)p_i[5] != G.N || (long long)p_i[6] != G.N * nf)
+    return fail(SS_ERR_ARG, "p_i[5]/p_i[6] (dim_grid/dim_fields) inconsistent with xlen*ylen*nf");
+  G.killkinen = p_i[7] ? 1 : 0;
+  G.unit_mag = p_i[9] ? 1 : 0;
+  G.lsx = p_f[2];
+  G.lsy = p_f[3];
+  G.dA = p_f[4];
+  G.dt = p_f[5];
+  G.ihx = 1.0 / G.lsx;
+  G.ihy = 1.0 / G.lsy;
+  G.ihx2 = 1.0 / (G.lsx * G.lsx);
+  G.ihy2 = 1.0 / (G.lsy * G.lsy);
+  G.ih2dA = 1.0 / (2.0 * G.dA);
+  if (!(G.lsx > 0) || !(G.lsy > 0) || !std::isfinite(G.lsx) || !std::isfinite(G.lsy) || !std::isfinite(G.dA) ||
+      !std::isfinite(G.dt))
+    return fail(SS_ERR_ARG, "lattice spacings / time step must be finite and positive");
+  h->nf = nf;
+  Phys& P = h->P;
+  memset(&P, 0, sizeof(P));
+  switch (theory) {
+    case SS_THEORY_CHIRAL_MAGNET: {
+      if (p_i[10] != 3) return fail(SS_ERR_ARG, "chiral magnet needs number_magnetization_fields=3");
+      P.c[0] = p_f[6];
+      P.c[1] = p_f[7];
+      P.c[2] = p_f[8];
+      double D00 = 0, D01 = 0, D10 = 0, D11 = 0;  // chiral_magnet/kernels.py:151-160
+      if (p_i[11]) {
+        D00 = -1.0; D11 = -1.0;
+      } else if (p_i[12]) {
+        D01 = -1.0; D10 = 1.0;
+      } else if (p_i[13]) {
+        D00 = 1.0; D11 = -1.0;
+      } else if (p_i[14]) {
+        const double s = 0.7071067811865476;
+        D00 = -s; D01 = -s; D10 = s; D11 = -s;
+      }
+      P.c[3] = D00; P.c[4] = D01; P.c[5] = D10; P.c[6] = D11;
+      P.k[0] = p_i[15] ? 1 : 0;
+      if (P.k[0] && !(P.c[2] != 0.0)) return fail(SS_ERR_ARG, "demag needs coup_mu != 0");
+      break;
+    }
+    case SS_THEORY_BABY_SKYRME: {
+      if (p_i[10] != 3) return fail(SS_ERR_ARG, "baby Skyrme needs number_magnetization_fields=3");
+      P.c[0] = p_f[6];
+      P.c[1] = p_f[7];
+      for (int i = 0; i < 8; ++i) P.k[i] = p_i[11 + i] ? 1 : 0;
+      P.k[8] = p_i[19];
+      if (P.k[6] && P.k[8] < 1) return fail(SS_ERR_ARG, "broken potential needs N >= 1");
+      break;
+    }
+    case SS_THEORY_GINZBURG_LANDAU: {
+      P.c[0] = p_f[6];
+      P.c[1] = p_f[7];
+      P.c[2] = p_f[8];
+      P.c[3] = p_f[9];
+      if (!(P.c[0] != 0.0)) return fail(SS_ERR_ARG, "q must be nonzero");
+      break;
+    }
+    case SS_THEORY_ANISOTROPIC: {
+      for (int i = 0; i < 11; ++i) P.c[i] = p_f[6 + i];
+      const double a1 = p_f[8], a2 = p_f[9], b1 = p_f[10], b2 = p_f[11], b3 = p_f[12], b4 = p_f[13];
+      const double u1 = p_f[17], u2 = p_f[18], th = p_f[19];
+      // vacuum energy density subtracted per site (anisotropic_superconductor/kernels.py:169)
+      P.c[11] = a1 * u1 * u1 + a2 * u2 * u2 + b1 * u1 * u1 * u1 * u1 + b2 * u2 * u2 * u2 * u2 + b3 * u1 * u1 * u2 * u2 +
+                2.0 * b4 * u1 * u1 * u2 * u2 * std::cos(2.0 * th);
+      if (!(P.c[1] != 0.0)) return fail(SS_ERR_ARG, "Q must be nonzero");
+      break;
+    }
+  }
+  return SS_OK;
+}
+
+int check_bound(const ss_handle* h) {
+  if (!h) return fail(SS_ERR_ARG, "NULL handle");
+  if (!h->ws) return fail(SS_ERR_STATE, "no workspace bound: call ss_bind first");
+  return SS_OK;
+}
+
+// Opt a kernel into more than 48 KB of dynamic shared memory, once per device.
+// `done` is owned by the caller's template instantiation.
+template <class K>
+void set_smem(K kernel, size_t bytes, unsigned long long& done) {
+  if (bytes <= 48 * 1024) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && (done >> dev) & 1ULL) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (dev < 64) done |= 1ULL << dev;
+}
+
+dim3 grid_1d(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return dim3((unsigned)b);
+}
+
+// ---------------------------------------------------------------------------
+// per-(theory, precision) implementation
+// ---------------------------------------------------------------------------
+template <class TH, typename R>
+struct Fused {
+  static constexpr size_t SMEM = tile_bytes<R, TH::NF, TX, TY>();
+
+  static inline unsigned long long smem_done_flow = 0, smem_done_density = 0;
+
+  static int launch(const ss_handle* h, const FlowArgs<R>& A) {
+    auto k = flow_kernel<TH, R, TX, TY, NT>;
+    set_smem(k, SMEM, smem_done_flow);
+    k<<<h->nblocks, NT, SMEM, h->stream>>>(A);
+    CK(cudaGetLastError());
+    return SS_OK;
+  }
+
+  static FlowArgs<R> base_args(const ss_handle* h) {
+    FlowArgs<R> A;
+    memset(&A, 0, sizeof(A));
+    A.G = h->G;
+    A.P = h->P;
+    A.st = h->st;
+    A.partial = h->partial;
+    A.E_idx = -1;
+    A.err_idx = -1;
+    A.prev_energy = NAN;
+    return A;
+  }
+
+  // n flow steps of the bound buffers; trajectories to device arrays (nullable)
+  static int step(ss_handle* h, int n, double prev, double* E_dev, double* err_dev) {
+    if (n <= 0) return SS_OK;
+    R* field = (R*)h->field;
+    R* vel = (R*)h->vel;
+    R* cur_p = field;
+    R* cur_v = vel;
+    R* alt_p = (R*)h->phi_alt;
+    R* alt_v = (R*)h->vel_alt;
+    R* l1 = (R*)h->l[0];
+    R* l2 = (R*)h->l[1];
+    R* l3 = (R*)h->l[2];
+    FlowArgs<R> A = base_args(h);
+    A.E_traj = E_dev;
+    A.err_traj = err_dev;
+    for (int s = 0; s < n; ++s) {
+      A.phi = cur_p;
+      A.vel = cur_v;
+      // S1: l1 = -dt G(phi); energy of phi (the previous step's result) + arrest test
+      A.mode = M_S1;
+      A.out_l = l1;
+      A.with_energy = s > 0;
+      A.arrest_update = s > 0;
+      A.E_idx = s - 1;
+      A.init_state = s == 0;
+      A.prev_energy = prev;
+      int rc = launch(h, A);
+      if (rc) return rc;
+      A.with_energy = 0;
+      A.arrest_update = 0;
+      A.init_state = 0;
+      A.E_idx = -1;
+      // S2, S3
+      A.mode = M_S2;
+      A.out_l = l2;
+      if ((rc = launch(h, A))) return rc;
+      A.mode = M_S3;
+      A.la = l1;
+      A.out_l = l3;
+      if ((rc = launch(h, A))) return rc;
+      // S4 + finalize into the ping-pong buffers
+      A.mode = M_S4;
+      A.la = l1;
+      A.lb = l2;
+      A.lc = l3;
+      A.out_l = nullptr;
+      A.phi_out = alt_p;
+      A.vel_out = alt_v;
+      A.err_idx = s;
+      if ((rc = launch(h, A))) return rc;
+      A.err_idx = -1;
+      std::swap(cur_p, alt_p);
+      std::swap(cur_v, alt_v);
+    }
+    // trailing energy of the final field + arrest test
+    A.phi = cur_p;
+    A.mode = M_ENERGY;
+    A.with_energy = 1;
+    A.arrest_update = 1;
+    A.E_idx = n - 1;
+    int rc = launch(h, A);
+    if (rc) return rc;
+    const long long nfN = (long long)h->nf * h->G.N;
+    finish_kernel<R><<<grid_1d(nfN), 256, 0, h->stream>>>(cur_p, cur_v, field, vel, nfN, cur_p != field ? 1 : 0,
+                                                          h->st);
+    CK(cudaGetLastError());
+    return SS_OK;
+  }
+
+  static int gradient(ss_handle* h, const void* field, void* eg, void* l_out) {
+    FlowArgs<R> A = base_args(h);
+    A.mode = M_GRAD;
+    A.phi = (const R*)field;
+    A.out_eg = (R*)eg;
+    A.out_l = (R*)l_out;
+    return launch(h, A);
+  }
+
+  static int energy(ss_handle* h, const void* field) {
+    FlowArgs<R> A = base_args(h);
+    A.mode = M_ENERGY;
+    A.phi = (const R*)field;
+    A.with_energy = 1;
+    return launch(h, A);
+  }
+
+  static int density(ss_handle* h, const void* field, double* dens, bool reduce, int kind, int which) {
+    auto k = density_kernel<TH, R, TX, TY, NT>;
+    set_smem(k, SMEM, smem_done_density);
+    k<<<h->nblocks, NT, SMEM, h->stream>>>((const R*)field, dens, reduce ? h->partial : nullptr, h->st, kind, which,
+                                           h->G, h->P);
+    CK(cudaGetLastError());
+    return SS_OK;
+  }
+
+  static int rk4_stage(ss_handle* h, void* k_out, const void* vel, const void* l_in, void* temp, const void* field,
+                       const void* k_prev, double factor) {
+    const long long n = (long long)h->nf * h->G.N;
+    rk4_stage_kernel<R><<<grid_1d(n), 256, 0, h->stream>>>((R*)k_out, (const R*)vel, (const R*)l_in, (R*)temp,
+                                                           (const R*)field, (const R*)k_prev, (R)factor, (R)h->G.dt, n);
+    CK(cudaGetLastError());
+    return SS_OK;
+  }
+
+  static int rk4_finalize(ss_handle* h, void* vel, void* field, const void* const* k, const void* const* l) {
+    rk4_finalize_kernel<R, TH::NF, TH::NMAG><<<grid_1d(h->G.N), 256, 0, h->stream>>>(
+        (R*)vel, (R*)field, (const R*)k[0], (const R*)k[1], (const R*)k[2], (const R*)k[3], (const R*)l[0],
+        (const R*)l[1], (const R*)l[2], (const R*)l[3], h->G.N, TH::CONSTRAINED && h->G.unit_mag);
+    CK(cudaGetLastError());
+    return SS_OK;
+  }
+};
+
+template <class TH>
+struct Plain {
+  static dim3 blocks(const ss_handle* h) { return dim3((h->G.X + 7) / 8, (h->G.Y + 7) / 8); }
+
+  static int gradient(ss_handle* h, const double* F, double* l_out, double* eg) {
+    plain_gradient_kernel<TH><<<blocks(h), dim3(8, 8), 0, h->stream>>>(l_out, F, h->d1, h->d2, eg, h->G, h->P);
+    CK(cudaGetLastError());
+    return SS_OK;
+  }
+
+  static int reduce(ss_handle* h, const double* var, long long size, int is_max, double* out) {
+    const int nb = (int)((size + 1023) / 1024);
+    plain_reduce_kernel<<<nb, 1024, 0, h->stream>>>(var, h->partial, size, is_max);
+    CK(cudaGetLastError());
+    h->host_partial.resize(nb);
+    CK(cudaMemcpyAsync(h->host_partial.data(), h->partial, nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    double r = is_max ? -INFINITY : 0.0;
+    for (int i = 0; i < nb; ++i) r = is_max ? std::max(r, h->host_partial[i]) : r + h->host_partial[i];
+    *out = r;
+    return SS_OK;
+  }
+
+  // observables.compute_energy (e.g. theories/chiral_magnet/observables.py:15-57)
+  static int energy(ss_handle* h, const double* F, double* out) {
+    plain_energy_kernel<TH><<<blocks(h), dim3(8, 8), 0, h->stream>>>(h->en, F, h->d1, h->G, h->P);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpyAsync(h->entmp, h->en, h->G.N * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    int rc = reduce(h, h->entmp, h->G.N, 0, out);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(h->entmp, 0, h->G.N * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(h->en, 0, h->G.N * sizeof(double), h->stream));
+    return SS_OK;
+  }
+
+  // do_arrested_newton_flow (core/integrator.py:217-348), one host-driven step at a time
+  static int step(ss_handle* h, int n, double prev, double* E_host, double* err_host) {
+    double* F = (double*)h->field;
+    double* V = (double*)h->vel;
+    double** k = (double**)h->k;
+    double** l = (double**)h->l;
+    double* T = (double*)h->temp;
+    double* EG = (double*)h->eg;
+    const long long nfN = (long long)h->nf * h->G.N;
+    double E = std::isnan(prev) ? h->E_last_host : prev;
+    const double factors[4] = {0.0, 0.5, 0.5, 1.0};
+    for (int s = 0; s < n; ++s) {
+      for (int st = 0; st < 4; ++st) {
+        const double* l_in = st == 0 ? V : l[st - 1];
+        const double* k_prev = st == 0 ? F : k[st - 1];
+        rk4_stage_kernel<double><<<grid_1d(nfN), 256, 0, h->stream>>>(k[st], V, l_in, T, F, k_prev, factors[st],
+                                                                          h->G.dt, nfN);
+        CK(cudaGetLastError());
+        int rc = gradient(h, T, l[st], EG);
+        if (rc) return rc;
+      }
+      rk4_finalize_kernel<double, TH::NF, TH::NMAG><<<grid_1d(h->G.N), 256, 0, h->stream>>>(
+          V, F, k[0], k[1], k[2], k[3], l[0], l[1], l[2], l[3], h->G.N, TH::CONSTRAINED && h->G.unit_mag);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(h->stream));
+      double E_new = 0.0;
+      int rc = energy(h, F, &E_new);
+      if (rc) return rc;
+      if (h->G.killkinen && E_new > E) {
+        CK(cudaMemsetAsync(V, 0, nfN * sizeof(double), h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+      }
+      double err = 0.0;
+      if ((rc = reduce(h, EG, nfN, 1, &err))) return rc;
+      E = E_new;
+      if (E_host) E_host[s] = E;
+      if (err_host) err_host[s] = err;
+      if (!std::isfinite(E)) {
+        h->E_last_host = E;
+        return fail(SS_ERR_NONFINITE, "non-finite energy at step %d", s);
+      }
+    }
+    h->E_last_host = E;
+    return SS_OK;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// dispatch tables
+// ---------------------------------------------------------------------------
+template <class Fn>
+int dispatch(const ss_handle* h, Fn&& fn) {
+  switch (h->theory) {
+    case SS_THEORY_CHIRAL_MAGNET: return fn((ChiralMagnet*)nullptr);
+    case SS_THEORY_BABY_SKYRME: return fn((BabySkyrme*)nullptr);
+    case SS_THEORY_GINZBURG_LANDAU: return fn((GinzburgLandau*)nullptr);
+    case SS_THEORY_ANISOTROPIC: return fn((Anisotropic*)nullptr);
+  }
+  return fail(SS_ERR_ARG, "bad theory");
+}
+
+int read_state(ss_handle* h, StepState* out) {
+  CK(cudaMemcpyAsync(out, h->st, sizeof(StepState), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return SS_OK;
+}
+
+int take_status(ss_handle* h) {
+  StepState s;
+  int rc = read_state(h, &s);
+  if (rc) return rc;
+  if (s.status) {
+    const int zero = 0;
+    CK(cudaMemcpyAsync(&h->st->status, &zero, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return fail(SS_ERR_NONFINITE, "a reduction produced a non-finite value");
+  }
+  return SS_OK;
+}
+
+int fused_density(ss_handle* h, const void* field, double* dens, bool reduce, int kind, int which) {
+  return dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (h->precision == SS_FP32) return Fused<TH, float>::density(h, field, dens, reduce, kind, which);
+    return Fused<TH, double>::density(h, field, dens, reduce, kind, which);
+  });
+}
+
+bool theory_has_charge(int theory, int which) {
+  switch (theory) {
+    case SS_THEORY_CHIRAL_MAGNET: return ChiralMagnet::has_charge(which);
+    case SS_THEORY_BABY_SKYRME: return BabySkyrme::has_charge(which);
+    case SS_THEORY_GINZBURG_LANDAU: return GinzburgLandau::has_charge(which);
+    case SS_THEORY_ANISOTROPIC: return Anisotropic::has_charge(which);
+  }
+  return false;
+}
+
+bool theory_has_coupling(int theory, int which) {
+  switch (theory) {
+    case SS_THEORY_CHIRAL_MAGNET: return ChiralMagnet::has_coupling(which);
+    case SS_THEORY_BABY_SKYRME: return BabySkyrme::has_coupling(which);
+    case SS_THEORY_GINZBURG_LANDAU: return GinzburgLandau::has_coupling(which);
+    case SS_THEORY_ANISOTROPIC: return Anisotropic::has_coupling(which);
+  }
+  return false;
+}
+
+int scalar_result(ss_handle* h, double* out) {
+  StepState s;
+  int rc = read_state(h, &s);
+  if (rc) return rc;
+  *out = s.scalar;
+  if (s.status) return take_status(h);
+  return SS_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// exported entry points
+// ===========================================================================
+extern "C" {
+
+int ss_abi_version(void) { return SS_ABI_VERSION; }
+
+const char* ss_status_string(int status) {
+  switch (status) {
+    case SS_OK: return "ok";
+    case SS_ERR_ARG: return "invalid argument";
+    case SS_ERR_CUDA: return "CUDA error";
+    case SS_ERR_NONFINITE: return "non-finite value";
+    case SS_ERR_STATE: return "invalid call order";
+    case SS_ERR_WORKSPACE: return "workspace too small or misaligned";
+  }
+  return "unknown status";
+}
+
+const char* ss_last_error(void) { return g_err; }
+
+int ss_create(int theory, const int32_t* p_i, int n_i, const double* p_f, int n_f, int precision, ss_handle** out) {
+  if (!out) return fail(SS_ERR_ARG, "out must not be NULL");
+  *out = nullptr;
+  if (precision != SS_FP64 && precision != SS_FP32 && precision != SS_PLAIN_FP64)
+    return fail(SS_ERR_ARG, "unknown precision %d", precision);
+  ss_handle* h = new ss_handle();
+  h->theory = theory;
+  h->precision = precision;
+  int rc = decode(h, theory, p_i, n_i, p_f, n_f);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  h->elem = precision == SS_FP32 ? 4 : 8;
+  const long long tiles = (long long)((h->G.X + TX - 1) / TX) * ((h->G.Y + TY - 1) / TY);
+  if (tiles > 0x7fffffffLL) {
+    delete h;
+    return fail(SS_ERR_ARG, "lattice too large");
+  }
+  h->nblocks = (int)tiles;
+  h->plain_sum_blocks = (int)((h->G.N + 1023) / 1024);
+  h->plain_max_blocks = (int)((h->G.N * h->nf + 1023) / 1024);
+  *out = h;
+  return SS_OK;
+}
+
+int ss_destroy(ss_handle* h) {
+  delete h;
+  return SS_OK;
+}
+
+int ss_workspace_bytes(const ss_handle* h, size_t* bytes) {
+  if (!h || !bytes) return fail(SS_ERR_ARG, "NULL argument");
+  ss_handle tmp = *h;
+  *bytes = layout(&tmp, nullptr);
+  return SS_OK;
+}
+
+int ss_bind(ss_handle* h, void* field, void* velocity, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!h) return fail(SS_ERR_ARG, "NULL handle");
+  if (!workspace) return fail(SS_ERR_ARG, "workspace must not be NULL");
+  if (((uintptr_t)workspace) % ALIGN) return fail(SS_ERR_WORKSPACE, "workspace must be %zu-byte aligned", ALIGN);
+  size_t need = 0;
+  ss_workspace_bytes(h, &need);
+  if (workspace_bytes < need) return fail(SS_ERR_WORKSPACE, "workspace has %zu bytes, needs %zu", workspace_bytes, need);
+  h->field = field;
+  h->vel = velocity;
+  h->ws = (char*)workspace;
+  h->ws_bytes = workspace_bytes;
+  h->stream = (cudaStream_t)stream;
+  layout(h, h->ws);
+  StepState init;
+  memset(&init, 0, sizeof(init));
+  init.E_last = NAN;
+  CK(cudaMemcpyAsync(h->st, &init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->E_last_host = NAN;
+  return SS_OK;
+}
+
+int ss_step_async(ss_handle* h, int n_steps, double prev_energy, double* energy_traj_dev, double* err_traj_dev) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (n_steps < 0) return fail(SS_ERR_ARG, "n_steps must be >= 0");
+  if (!h->field || !h->vel) return fail(SS_ERR_STATE, "no Field/Velocity bound");
+  if (h->precision == SS_PLAIN_FP64)
+    return fail(SS_ERR_ARG, "the plain FP64 form arrests on the host; use ss_step");
+  return dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (h->precision == SS_FP32) return Fused<TH, float>::step(h, n_steps, prev_energy, energy_traj_dev, err_traj_dev);
+    return Fused<TH, double>::step(h, n_steps, prev_energy, energy_traj_dev, err_traj_dev);
+  });
+}
+
+int ss_step(ss_handle* h, int n_steps, double prev_energy, double* energy_traj, double* err_traj) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (n_steps < 0) return fail(SS_ERR_ARG, "n_steps must be >= 0");
+  if (!h->field || !h->vel) return fail(SS_ERR_STATE, "no Field/Velocity bound");
+  if (h->precision == SS_PLAIN_FP64) {
+    return dispatch(h, [&](auto* tag) -> int {
+      using TH = std::remove_pointer_t<decltype(tag)>;
+      return Plain<TH>::step(h, n_steps, prev_energy, energy_traj, err_traj);
+    });
+  }
+  double prev = prev_energy;
+  for (int done = 0; done < n_steps; done += TRAJ_CAP) {
+    const int k = std::min(TRAJ_CAP, n_steps - done);
+    rc = ss_step_async(h, k, prev, h->traj_E, h->traj_err);
+    if (rc) return rc;
+    prev = NAN;
+    if (energy_traj)
+      CK(cudaMemcpyAsync(energy_traj + done, h->traj_E, k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (err_traj)
+      CK(cudaMemcpyAsync(err_traj + done, h->traj_err, k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  }
+  return take_status(h);
+}
+
+int ss_check_status(ss_handle* h) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  return take_status(h);
+}
+
+int ss_gradient(ss_handle* h, const void* field, void* energy_gradient, void* l_out) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!field) return fail(SS_ERR_ARG, "field must not be NULL");
+  if (h->precision == SS_PLAIN_FP64) {
+    return dispatch(h, [&](auto* tag) -> int {
+      using TH = std::remove_pointer_t<decltype(tag)>;
+      double* eg = energy_gradient ? (double*)energy_gradient : (double*)h->eg;
+      double* l = l_out ? (double*)l_out : (double*)h->l[0];
+      return Plain<TH>::gradient(h, (const double*)field, l, eg);
+    });
+  }
+  return dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (h->precision == SS_FP32) return Fused<TH, float>::gradient(h, field, energy_gradient, l_out);
+    return Fused<TH, double>::gradient(h, field, energy_gradient, l_out);
+  });
+}
+
+int ss_energy_density(ss_handle* h, const void* field, double* density) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!field || !density) return fail(SS_ERR_ARG, "NULL argument");
+  return fused_density(h, field, density, false, D_ENERGY, 0);
+}
+
+int ss_energy(ss_handle* h, const void* field, double* out) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!field || !out) return fail(SS_ERR_ARG, "NULL argument");
+  if (h->precision == SS_PLAIN_FP64) {
+    return dispatch(h, [&](auto* tag) -> int {
+      using TH = std::remove_pointer_t<decltype(tag)>;
+      return Plain<TH>::energy(h, (const double*)field, out);
+    });
+  }
+  rc = dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (h->precision == SS_FP32) return Fused<TH, float>::energy(h, field);
+    return Fused<TH, double>::energy(h, field);
+  });
+  if (rc) return rc;
+  return scalar_result(h, out);
+}
+
+int ss_charge_density(ss_handle* h, const void* field, int which, double* density) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!field || !density) return fail(SS_ERR_ARG, "NULL argument");
+  if (!theory_has_charge(h->theory, which)) return fail(SS_ERR_ARG, "charge %d not defined for theory %d", which, h->theory);
+  return fused_density(h, field, density, false, D_CHARGE, which);
+}
+
+int ss_charge(ss_handle* h, const void* field, int which, double* out) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!field || !out) return fail(SS_ERR_ARG, "NULL argument");
+  if (!theory_has_charge(h->theory, which)) return fail(SS_ERR_ARG, "charge %d not defined for theory %d", which, h->theory);
+  rc = fused_density(h, field, nullptr, true, D_CHARGE, which);
+  if (rc) return rc;
+  return scalar_result(h, out);
+}
+
+int ss_coupling_grad(ss_handle* h, const void* field, int coupling, double* out) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!field || !out) return fail(SS_ERR_ARG, "NULL argument");
+  if (!theory_has_coupling(h->theory, coupling))
+    return fail(SS_ERR_ARG, "coupling %d not defined for theory %d", coupling, h->theory);
+  rc = fused_density(h, field, nullptr, true, D_COUPLING, coupling);
+  if (rc) return rc;
+  return scalar_result(h, out);
+}
+
+int ss_rk4_stage(ss_handle* h, void* k_out, const void* velocity, const void* l_in, void* temp, const void* field,
+                 const void* k_prev, double factor) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!k_out || !velocity || !l_in || !temp || !field || !k_prev) return fail(SS_ERR_ARG, "NULL argument");
+  return dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (h->precision == SS_FP32) return Fused<TH, float>::rk4_stage(h, k_out, velocity, l_in, temp, field, k_prev, factor);
+    return Fused<TH, double>::rk4_stage(h, k_out, velocity, l_in, temp, field, k_prev, factor);
+  });
+}
+
+int ss_rk4_finalize(ss_handle* h, void* velocity, void* field, const void* k1, const void* k2, const void* k3,
+                    const void* k4, const void* l1, const void* l2, const void* l3, const void* l4) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  const void* k[4] = {k1, k2, k3, k4};
+  const void* l[4] = {l1, l2, l3, l4};
+  for (int i = 0; i < 4; ++i)
+    if (!k[i] || !l[i]) return fail(SS_ERR_ARG, "NULL argument");
+  if (!velocity || !field) return fail(SS_ERR_ARG, "NULL argument");
+  return dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (h->precision == SS_FP32) return Fused<TH, float>::rk4_finalize(h, velocity, field, k, l);
+    return Fused<TH, double>::rk4_finalize(h, velocity, field, k, l);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,15 @@
+"""Hook adapters of the Anisotropic superconductor theory.
+
+Same hook names and call signatures as soliton_solver/theories/anisotropic_superconductor/kernels.py;
+every call runs the hand-written sm_100a kernels of libsoliton_b200.
+"""
+from soliton_solver_b200 import _native as _nat
+from soliton_solver_b200.core.hooks import make_kernels
+
+THEORY_ID = _nat.SS_THEORY_ANISOTROPIC
+CHARGES = ('vortex',)
+CONSTRAINED = False
+
+globals().update(make_kernels(THEORY_ID, CHARGES))
+
+del do_rk4_kernel  # unconstrained: Simulation uses the core no-constraint finalize

@@ -1,0 +1,87 @@
+"""The C ABI library loads, exports every function include/soliton_b200.h declares,
+and validates its arguments on the host (no kernel launch, no GPU needed)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from soliton_solver_b200 import _native as nat
+from soliton_solver_b200.theories import load_theory
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "soliton_b200.h")
+
+
+def _declared():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*)\s*(ss_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = nat.load()
+    names = _declared()
+    assert len(names) >= 18
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(nat.EXPORTS)
+    assert lib.ss_abi_version() == 1
+
+
+def _create(theory_name, **kw):
+    th = load_theory(theory_name)
+    p_i, p_f = th.params.pack_device_params(th.params.default_params(**kw).resolved())
+    h = ctypes.c_void_p()
+    rc = nat.load().ss_create(th.kernels.THEORY_ID, p_i.ctypes.data, len(p_i), p_f.ctypes.data, len(p_f),
+                              nat.SS_FP32, ctypes.byref(h))
+    return rc, h, p_i, p_f
+
+
+def test_create_and_workspace_size():
+    lib = nat.load()
+    rc, h, p_i, p_f = _create("Chiral magnet", xlen=100, ylen=70, demag=True)
+    assert rc == 0
+    n = ctypes.c_size_t()
+    assert lib.ss_workspace_bytes(h, ctypes.byref(n)) == 0
+    # l1..l3 and the ping-pong Field/Velocity copies: 5 FP32 field-sized buffers at least
+    assert n.value >= 5 * 4 * 4 * 100 * 70
+    assert lib.ss_destroy(h) == 0
+
+
+@pytest.mark.parametrize("mutate,msg", [
+    (lambda pi, pf: pi.__setitem__(2, 1), "halo"),
+    (lambda pi, pf: pi.__setitem__(4, 3), "number_total_fields"),
+    (lambda pi, pf: pi.__setitem__(5, 7), "dim_grid"),
+    (lambda pi, pf: pf.__setitem__(2, -1.0), "spacings"),
+    (lambda pi, pf: pi.__setitem__(3, 3), "number_coordinates"),
+])
+def test_create_rejects_bad_params(mutate, msg):
+    lib = nat.load()
+    th = load_theory("Chiral magnet")
+    p_i, p_f = th.params.pack_device_params(th.params.default_params(xlen=20, ylen=20).resolved())
+    mutate(p_i, p_f)
+    h = ctypes.c_void_p()
+    rc = lib.ss_create(0, p_i.ctypes.data, len(p_i), p_f.ctypes.data, len(p_f), nat.SS_FP32, ctypes.byref(h))
+    assert rc == nat.SS_ERR_ARG
+    assert msg in lib.ss_last_error().decode()
+    with pytest.raises(ValueError):
+        nat.check(rc)
+
+
+def test_calls_before_bind_are_rejected():
+    lib = nat.load()
+    rc, h, _, _ = _create("Baby Skyrme", xlen=16, ylen=16)
+    assert rc == 0
+    assert lib.ss_step(h, 1, 0.0, None, None) == nat.SS_ERR_STATE
+    assert lib.ss_gradient(h, None, None, None) == nat.SS_ERR_STATE
+    lib.ss_destroy(h)
+
+
+def test_short_param_arrays_and_bad_ids():
+    lib = nat.load()
+    h = ctypes.c_void_p()
+    p_i = np.zeros(4, np.int32)
+    p_f = np.zeros(4)
+    assert lib.ss_create(0, p_i.ctypes.data, 4, p_f.ctypes.data, 4, 1, ctypes.byref(h)) == nat.SS_ERR_ARG
+    assert lib.ss_create(9, p_i.ctypes.data, 4, p_f.ctypes.data, 4, 1, ctypes.byref(h)) == nat.SS_ERR_ARG
+    assert lib.ss_create(0, p_i.ctypes.data, 4, p_f.ctypes.data, 4, 7, ctypes.byref(h)) == nat.SS_ERR_ARG

@@ -1,0 +1,84 @@
+"""Pin the FP64 oracle to golden vectors produced by the reference itself.
+
+The fixtures in ``tests/golden`` were written by ``tests/golden/make_golden.py``,
+which runs the reference's own Numba kernels (under Numba's CUDA simulator) on
+seeded random fields.  The oracle restates those kernels in the same operation
+order, so agreement is expected to the last few ulps.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import flow64 as ref
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+HOOKS = sorted(glob.glob(os.path.join(GOLDEN, "hook_*.npz")))
+TRAJS = sorted(glob.glob(os.path.join(GOLDEN, "traj_*.npz")))
+
+# Relative to the largest magnitude of the compared array: the oracle follows the
+# reference's association order, so the only differences are libm ulps.
+RTOL = 1e-13
+
+
+def _close(a, b, rtol=RTOL):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = max(1.0, float(np.max(np.abs(b)))) if b.size else 1.0
+    err = float(np.max(np.abs(a - b))) if b.size else 0.0
+    assert err <= rtol * scale, f"max abs err {err:.3e} > {rtol:.1e} * {scale:.3e}"
+
+
+def test_fixtures_present():
+    assert len(HOOKS) >= 20 and len(TRAJS) >= 5
+
+
+@pytest.mark.parametrize("path", HOOKS, ids=[os.path.basename(p)[5:-4] for p in HOOKS])
+def test_hooks(path):
+    g = np.load(path)
+    th = str(g["theory"])
+    p_i, p_f = g["p_i"], g["p_f"]
+    F = ref.as_field(g["field"], p_i)
+    V = ref.as_field(g["velocity"], p_i)
+    l_out, EG = ref.gradient_step(th, F, p_i, p_f)
+    _close(EG.reshape(-1), g["energy_gradient"])
+    _close(l_out.reshape(-1), g["l_out"])
+    _close(ref.energy_density(th, F, p_i, p_f).reshape(-1), g["energy_density"])
+    E = ref.energy(th, F, p_i, p_f)
+    assert abs(E - float(g["energy"])) <= 1e-13 * max(1.0, abs(float(g["energy"])))
+    assert abs(E - float(g["obs_energy"])) <= 1e-13 * max(1.0, abs(float(g["energy"])))
+    if "skyrmion_density" in g:
+        d = ref.charge_density(th, F, p_i, p_f, "skyrmion")
+        _close(d.reshape(-1), g["skyrmion_density"])
+        assert abs(ref.reference_sum(d) - float(g["obs_skyrmion_number"])) <= 1e-13
+    if "magnetic_charge_density" in g:
+        d = ref.charge_density(th, F, p_i, p_f, "magnetic")
+        _close(d.reshape(-1), g["magnetic_charge_density"])
+        assert abs(ref.reference_sum(d) - float(g["obs_magnetic_charge"])) <= 1e-13
+    if "vortex_density" in g:
+        d = ref.charge_density(th, F, p_i, p_f, "vortex")
+        _close(d.reshape(-1), g["vortex_density"])
+        assert abs(ref.reference_sum(d) - float(g["obs_vortex_number"])) <= 1e-13
+    ks = [ref.as_field(k, p_i) for k in g["rk4_k"]]
+    ls = [ref.as_field(v, p_i) for v in g["rk4_l"]]
+    k_out, temp = ref.rk4_stage(V, ls[0], F, ks[0], 0.5, p_f)
+    _close(k_out.reshape(-1), g["rk4_stage_k_out"])
+    _close(temp.reshape(-1), g["rk4_stage_temp"])
+    Vn, Fn = ref.rk4_finalize(th, V, F, *ks, *ls, p_i)
+    _close(Vn.reshape(-1), g["rk4_final_velocity"])
+    _close(Fn.reshape(-1), g["rk4_final_field"])
+
+
+@pytest.mark.parametrize("path", TRAJS, ids=[os.path.basename(p)[:-4] for p in TRAJS])
+def test_trajectories(path):
+    g = np.load(path)
+    th = str(g["theory"])
+    p_i, p_f = g["p_i"], g["p_f"]
+    F = ref.as_field(g["field"], p_i)
+    V = ref.as_field(g["velocity"], p_i)
+    F, V, E, err = ref.relax(th, F, V, float(g["prev_energy"]), p_i, p_f, int(g["n_steps"]))
+    np.testing.assert_allclose(E, g["energy_traj"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(err, g["err_traj"], rtol=1e-12, atol=1e-14)
+    _close(F.reshape(-1), g["final_field"], 1e-12)
+    _close(V.reshape(-1), g["final_velocity"], 1e-12)
