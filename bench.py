@@ -1,0 +1,393 @@
+"""Benchmark: arrested-Newton-flow relaxation throughput of a 4096^2 chiral magnet.
+
+Workload (one "step" = one full RK4 arrested-Newton-flow step of the whole lattice):
+chiral magnet, 4096 x 4096 sites over a 128 x 128 reduced domain (lsx = 128/4095),
+J = 40e-12, K = 0.8e6, D = 4e-3, M = 580e3, B = 0.2 T, Heusler DMI, demag on (psi
+relaxed as the 4th field), unit magnetisation, killkinen off (plain RK4 gradient
+flow), FP32 fields with FP64 energy reductions.  Initial field: 64 anti-skyrmions at
+seeded jittered 8 x 8 lattice positions plus N(0, 1e-3) noise (synthetic; the
+reference has no dataset).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank relaxes its own lattice (independent replicas, no
+data-path collective: weak scaling); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+XLEN = YLEN = 4096
+XSIZE = 128.0
+METRIC = "Mpoint-updates/s per flow step at dE/E<=1e-6 vs plain FP64; achieved HBM GB/s"
+UNIT = "Mpoint-updates/s"
+WORDS_PER_SITE_STEP = 16  # S1: 2, S2: 3, S3: 4, S4: 7 words of nf components
+
+
+def chiral_params(xlen=None, ylen=None, xsize=None):
+    from soliton_solver_b200.theories import load_theory
+    xlen, ylen, xsize = xlen or XLEN, ylen or YLEN, xsize or XSIZE
+    th = load_theory("Chiral magnet")
+    p = th.params.default_params(xlen=xlen, ylen=ylen, xsize=xsize, ysize=xsize * (ylen - 1) / (xlen - 1) if xlen > 1
+                                 else xsize, J=40e-12, K=0.8e6, D=4e-3, M=580e3, B=0.2, dmi_term="Heusler",
+                                 demag=True, unit_magnetization=True, killkinen=False)
+    return th, p
+
+
+def config(extra=None):
+    c = {"workload": "chiral magnet 4096x4096, Heusler DMI, demag on, B=0.2 T, 64-skyrmion lattice, RK4 flow",
+         "theory": "Chiral magnet", "xlen": XLEN, "ylen": YLEN, "nf": 4, "fields": "fp32", "reductions": "fp64",
+         "l2": "no flush: working set 1.6 GB per step >> 126 MB L2"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi sampler (20 ms period); summary() keeps the samples between the
+    first and last mark() (the timed region)."""
+
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.marks = []
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def mark(self):
+        """Record the wall time of a timed-region boundary."""
+        self.marks.append(time.time())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        import datetime
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        lo, hi = (self.marks[0], self.marks[-1]) if len(self.marks) >= 2 else (-math.inf, math.inf)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path).read().strip().splitlines():
+            r = [x.strip() for x in line.split(",")]
+            if len(r) < 10:
+                continue
+            try:
+                t = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                if not (lo <= t <= hi):
+                    continue
+                sm.append(float(r[2]))
+                smax.append(float(r[3]))
+                power.append(float(r[4]))
+            except ValueError:
+                continue
+            for n, v in zip(names, r[6:10]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU leg: the FP64 oracle on bounded stripes, one thread per stripe
+# ---------------------------------------------------------------------------
+def cpu_sample(steps, warmup, threads=None, rows=128):
+    """Time the oracle's flow step on ``threads`` independent rows x 4096 stripes of the
+    workload (each a Dirichlet sub-lattice with the workload's spacing); returns
+    point-updates/s and a description."""
+    from oracle import flow64 as ref
+    from soliton_solver_b200.initial_conditions import skyrmion_lattice
+    threads = threads or min(os.cpu_count() or 1, 16)
+    th, p = chiral_params(rows, YLEN, XSIZE * (rows - 1) / (XLEN - 1))
+    p = p.with_(ysize=XSIZE)
+    rp = p.resolved()
+    p_i, p_f = th.params.pack_device_params(rp)
+    F0 = skyrmion_lattice(rp, n=1, R=1.0, seed=0).numpy().reshape(4, rows, YLEN)
+    V0 = np.zeros_like(F0)
+
+    def run(n):
+        F, V = F0.copy(), V0.copy()
+        ref.relax("chiral_magnet", F, V, 1e300, p_i, p_f, n)
+
+    with cf.ThreadPoolExecutor(threads) as ex:
+        for _ in range(warmup):
+            list(ex.map(run, [1] * threads))
+        t = time.perf_counter()
+        for _ in range(steps):
+            list(ex.map(run, [1] * threads))
+        dt = (time.perf_counter() - t) / max(steps, 1)
+    value = threads * rows * YLEN / dt / 1e6
+    sample = (f"{threads} independent {rows}x{YLEN} stripes of the workload (FP64 numpy oracle restating the "
+              f"reference kernels), 1 flow step each per timed step")
+    return value, threads, sample, dt
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    steps, warmup = max(args.steps, 1), max(args.warmup, 0)
+    value, threads, sample, dt = cpu_sample(min(steps, 3), min(warmup, 1))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": min(steps, 3),
+            "warmup": min(warmup, 1), "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config({"sample": sample}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from soliton_solver_b200.core.simulation import Simulation
+    from soliton_solver_b200.initial_conditions import skyrmion_lattice
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    th, p = chiral_params()
+    sim = Simulation(p, th, precision="fp32", device=dev)
+    F0 = skyrmion_lattice(sim.rp, n=8, R=1.0, seed=1000 + rank, device=dev)
+    sim.load_field(F0)
+    s = sim.solver
+    stream = torch.cuda.current_stream(dev)
+    N = XLEN * YLEN
+    K, W = args.steps, args.warmup
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    E_traj = torch.empty(K, dtype=torch.float64, device=dev)
+    err_traj = torch.empty(K, dtype=torch.float64, device=dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        # warm-up (untimed); also gives the clock sampler time to start
+        s.step(max(W, 1), 1e300)
+        time.sleep(0.5)
+        barrier()
+        torch.cuda.synchronize(dev)
+        clk.mark()
+        ev0.record(stream)
+        s.step_async(K, math.nan, E_traj, err_traj)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        clk.mark()
+    s.check_status()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    ms_step = ms / K
+    value = world * N * K / (ms / 1e3) / 1e6
+    launches = 4 * K + 2
+
+    # roofline of the fused stage kernel (4 launches per step)
+    from soliton_solver_b200._native import load as _load  # noqa: F401 (library loaded)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    bytes_step = WORDS_PER_SITE_STEP * 4 * 4 * N
+    achieved = bytes_step / (ms_step / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "flow_kernel_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch_at_4096")
+        except Exception:
+            traffic = None
+
+    # end to end through the reference-facing API: host field in (pinned), one
+    # Simulation.step(E) per step returning (E, err) to the host, host field out.
+    host_F = F0.to(torch.float32).cpu().pin_memory()
+    host_V = torch.zeros_like(host_F).pin_memory()
+    out_F = torch.empty_like(host_F).pin_memory()
+    Ke = max(K // 2, 3)
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    sim.Field.copy_(host_F, non_blocking=True)
+    sim.Velocity.copy_(host_V, non_blocking=True)
+    E = 1e300
+    for _ in range(Ke):
+        E, err = sim.step(E)
+    out_F.copy_(sim.Field, non_blocking=True)
+    torch.cuda.synchronize(dev)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * N * Ke / e2e_s / 1e6
+    h2d = (host_F.numel() + host_V.numel()) * 4 / Ke
+    d2h = out_F.numel() * 4 / Ke + 16
+
+    extra = {}
+    if rank == 0 and not args.no_compare:
+        extra = compare_fp64_and_plain(args, dev, F0)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, threads, sample, _ = cpu_sample(1, 0)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+                "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 fields / f64 reductions", "data": "synthetic",
+                "config": config({"parallelism": f"replicas x{world}" if world > 1 else "single lattice",
+                                  "global_sites": world * N}),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                             "kernel": "flow_kernel<ChiralMagnet,float> (4 stage launches per step)",
+                             "algorithmic_bytes_per_step": bytes_step},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "steps": Ke, "api": "Simulation.step(prev_energy) per step"},
+                "gpu_launches": launches, "clocks": clk.summary()}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def relaxed_accuracy(dev, max_steps=20000, chunk=1000, tol=1e-6):
+    """The 320^2 chiral magnet (10 x 10 reduced domain, Heusler DMI, demag off, B = 0,
+    arrested Newton flow) relaxed from an anti-skyrmion in FP32, fused FP64 and the
+    plain FP64 form; reports relaxed energies, charges and the FP32 / FP64 gap."""
+    import torch
+    from soliton_solver_b200.core.simulation import Simulation
+    from soliton_solver_b200.initial_conditions import anti_skyrmion
+    from soliton_solver_b200.theories import load_theory
+    th = load_theory("Chiral magnet")
+    p = th.params.default_params(xlen=320, ylen=320, xsize=10.0, ysize=10.0, J=40e-12, K=0.8e6, D=4e-3, M=580e3,
+                                 B=0.0, dmi_term="Heusler", demag=False, unit_magnetization=True, killkinen=True)
+    out = {"config": "chiral magnet 320x320 over 10x10 J/D, Heusler, demag off, B=0, anti-skyrmion R=1 + "
+                     "N(0,1e-3), arrested Newton flow until max dE/dphi < 1e-6 or 20000 steps"}
+    for prec in ("fp64", "fp32", "plain_fp64"):
+        sim = Simulation(p, th, precision=prec, device=dev)
+        sim.load_field(anti_skyrmion(sim.rp, R=1.0, sigma=1e-3, seed=0, device=dev))
+        E = sim.observables()["energy"]
+        steps, err = 0, math.inf
+        t0 = time.perf_counter()
+        while steps < max_steps:
+            n = chunk if prec != "plain_fp64" else max_steps
+            Es, errs = sim.relax(n, E if steps == 0 else math.nan)
+            steps += n
+            E, err = float(Es[-1]), float(errs[-1])
+            if abs(err) < tol:
+                break
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - t0
+        obs = sim.observables()
+        out[prec] = {"E": E, "Q": obs["skyrmion_number"], "err": err, "steps": steps, "wall_s": wall}
+        del sim
+        torch.cuda.empty_cache()
+    e64, e32 = out["fp64"]["E"], out["fp32"]["E"]
+    out["rel_diff_fp32_vs_fp64"] = abs(e32 - e64) / abs(e64)
+    out["rel_diff_fp64_vs_plain"] = abs(e64 - out["plain_fp64"]["E"]) / abs(out["plain_fp64"]["E"])
+    out["charge_dev_from_integer_fp32"] = abs(out["fp32"]["Q"] - round(out["fp32"]["Q"]))
+    return out
+
+
+def compare_fp64_and_plain(args, dev, F0):
+    """Relaxed-state accuracy (320^2), and the plain-FP64 form's speed on this lattice."""
+    import torch
+    from soliton_solver_b200.core.simulation import Simulation
+    th, p = chiral_params()
+    out = {"accuracy": relaxed_accuracy(dev)}
+    sim = Simulation(p, th, precision="plain_fp64", device=dev)
+    sim.load_field(F0)
+    sim.relax(1, 1e300)
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter()
+    kp = 3
+    sim.relax(kp, math.nan)
+    torch.cuda.synchronize(dev)
+    dt = (time.perf_counter() - t) / kp
+    out["plain_fp64"] = {"value": XLEN * YLEN / dt / 1e6, "unit": UNIT, "ms_per_step": dt * 1e3,
+                         "note": "reference-structured FP64 CUDA form (derivative buffers, per-stage launches, "
+                                 "host-side arrest), same lattice"}
+    del sim
+    torch.cuda.empty_cache()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 / plain-FP64 comparison")
+    ap.add_argument("--size", type=int, default=4096, help="lattice edge (4096 is the workload; smaller sizes "
+                                                             "are for profiler captures)")
+    args = ap.parse_args()
+    global XLEN, YLEN, XSIZE
+    if args.size != 4096:
+        XLEN = YLEN = args.size
+        XSIZE = 128.0 * (args.size - 1) / 4095
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        return gpu_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -42,6 +42,7 @@ extern "C" {
 #define SS_ERR_NONFINITE 3    /* a reduction produced NaN or Inf */
 #define SS_ERR_STATE 4        /* call out of order (e.g. no workspace bound) */
 #define SS_ERR_WORKSPACE 5    /* workspace too small or misaligned */
+#define SS_ERR_TIMEOUT 6      /* a bounded device-side wait expired (kernel returned early) */
 
 /* theories (THEORY_SPEC names of the reference theory packages) */
 #define SS_THEORY_CHIRAL_MAGNET 0   /* theories/chiral_magnet */
@@ -60,13 +61,16 @@ extern "C" {
 #define SS_CHARGE_MAGNETIC 1 /* -div m dA : chiral magnet */
 #define SS_CHARGE_VORTEX 2   /* (dx A2 - dy A1) dA/(2 pi q) : Ginzburg-Landau, s+id */
 
-/* couplings for ss_coupling_grad (partial derivatives of E at fixed field) */
-#define SS_COUPLING_KAPPA 0  /* baby Skyrme kappa */
-#define SS_COUPLING_MPI 1    /* baby Skyrme mpi */
-#define SS_COUPLING_LAMBDA 2 /* Ginzburg-Landau Lambda */
-#define SS_COUPLING_B 3      /* chiral magnet applied field B (through coup_h) */
-#define SS_COUPLING_D 4      /* chiral magnet DMI strength D (through coup_K, coup_h, coup_mu) */
-#define SS_COUPLING_K 5      /* chiral magnet anisotropy K (through coup_K) */
+/* couplings for ss_coupling_grad (partial derivatives of E at fixed field).  The
+ * chiral magnet's physical constants enter only through the reduced couplings
+ * coup_K = K J/D^2, coup_h = M B J/D^2, coup_mu = mu0 M^2 J/D^2; the host applies
+ * the chain rule for dE/dB, dE/dK, dE/dD. */
+#define SS_COUPLING_KAPPA 0   /* baby Skyrme kappa */
+#define SS_COUPLING_MPI 1     /* baby Skyrme mpi */
+#define SS_COUPLING_LAMBDA 2  /* Ginzburg-Landau Lambda */
+#define SS_COUPLING_COUP_K 3  /* chiral magnet coup_K (p_f[6]) */
+#define SS_COUPLING_COUP_H 4  /* chiral magnet coup_h (p_f[7]) */
+#define SS_COUPLING_COUP_MU 5 /* chiral magnet coup_mu (p_f[8]) */
 
 typedef struct ss_handle ss_handle;
 
@@ -101,6 +105,9 @@ int ss_step_async(ss_handle *h, int n_steps, double prev_energy, double *energy_
                   double *err_traj_dev);
 /* Synchronise the bound stream and return the status the device-side checks set. */
 int ss_check_status(ss_handle *h);
+/* 1 when the bound Field/Velocity/workspace buffers are staged by TMA tensor maps
+ * (row pitch and base 16-byte aligned), 0 when the plain-load path is used. */
+int ss_tma_enabled(const ss_handle *h);
 
 /* One gradient evaluation of an arbitrary field buffer: energy_gradient (nullable)
  * receives the theory's projected dE/dphi, l_out (nullable) receives -dt*dE/dphi.

@@ -18,6 +18,7 @@ SS_ERR_CUDA = 2
 SS_ERR_NONFINITE = 3
 SS_ERR_STATE = 4
 SS_ERR_WORKSPACE = 5
+SS_ERR_TIMEOUT = 6
 
 # theories
 SS_THEORY_CHIRAL_MAGNET = 0
@@ -73,6 +74,7 @@ _SIG = {
     "ss_step": ([_P, _I, _D, _P, _P], _I),
     "ss_step_async": ([_P, _I, _D, _P, _P], _I),
     "ss_check_status": ([_P], _I),
+    "ss_tma_enabled": ([_P], _I),
     "ss_gradient": ([_P, _P, _P, _P], _I),
     "ss_energy_density": ([_P, _P, _P], _I),
     "ss_energy": ([_P, _P, ctypes.POINTER(_D)], _I),

@@ -115,6 +115,11 @@ class Solver:
             nat.check(self._lib.ss_step_async(self._h, int(n_steps), float(prev_energy), _ptr(energy_traj),
                                               _ptr(err_traj)))
 
+    @property
+    def tma_enabled(self) -> bool:
+        """True when the bound buffers are staged with TMA tensor maps."""
+        return bool(self._lib.ss_tma_enabled(self._h))
+
     def check_status(self):
         nat.check(self._lib.ss_check_status(self._h))
 

@@ -7,6 +7,9 @@
 #include <cstring>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "../../include/soliton_b200.h"
 #include "common.cuh"
 #include "flow.cuh"
@@ -38,6 +41,38 @@ int fail(int code, const char* fmt, ...) {
   } while (0)
 
 size_t align_up(size_t v) { return (v + ALIGN - 1) / ALIGN * ALIGN; }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// 3-D map over component planes (dims y, x, component) whose box is one staged
+// tile: (TY + 8) x (TX + 4) x NF.  Fails (-> plain loads) when the buffer or its
+// row pitch is not 16-byte aligned.
+bool encode_tile_map(CUtensorMap* m, const void* ptr, size_t es, int X, int Y, int NF) {
+  if (!ptr || ((uintptr_t)ptr) % 16 || ((size_t)Y * es) % 16) return false;
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)Y, (cuuint64_t)X, (cuuint64_t)NF};
+  cuuint64_t strides[2] = {(cuuint64_t)Y * es, (cuuint64_t)X * Y * es};
+  cuuint32_t box[3] = {(cuuint32_t)(TY + 8), (cuuint32_t)(TX + 4), (cuuint32_t)NF};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(m, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                  const_cast<void*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
 
 }  // namespace
 
@@ -72,6 +107,9 @@ struct ss_handle {
   double* entmp = nullptr;
   double E_last_host = NAN;
   std::vector<double> host_partial;
+  // TMA maps of the bound buffers: field, velocity, phi_alt, vel_alt, l1, l2
+  CUtensorMap tm[6];
+  bool tma = false;
 };
 
 namespace {
@@ -215,7 +253,7 @@ int check_bound(const ss_handle* h) {
 // `done` is owned by the caller's template instantiation.
 template <class K>
 void set_smem(K kernel, size_t bytes, unsigned long long& done) {
-  if (bytes <= 48 * 1024) return;
+  if (bytes <= 32 * 1024) return;
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && (done >> dev) & 1ULL) return;
@@ -235,14 +273,20 @@ dim3 grid_1d(long long n) {
 // ---------------------------------------------------------------------------
 template <class TH, typename R>
 struct Fused {
-  static constexpr size_t SMEM = tile_bytes<R, TH::NF, TX, TY>();
+  static constexpr size_t BUF = tile_buf_bytes<R, TH::NF, TX, TY>();
+  static inline unsigned long long smem_done_flow = 0, smem_done_tma = 0, smem_done_density = 0;
 
-  static inline unsigned long long smem_done_flow = 0, smem_done_density = 0;
-
-  static int launch(const ss_handle* h, const FlowArgs<R>& A) {
-    auto k = flow_kernel<TH, R, TX, TY, NT>;
-    set_smem(k, SMEM, smem_done_flow);
-    k<<<h->nblocks, NT, SMEM, h->stream>>>(A);
+  // tma: use the TMA-staged instantiation (A.tm_* must describe A's buffers)
+  static int launch(const ss_handle* h, const FlowArgs<R>& A, bool tma) {
+    if (tma) {
+      auto k = flow_kernel<TH, R, TX, TY, NT, true>;
+      set_smem(k, 3 * BUF, smem_done_tma);
+      k<<<h->nblocks, NT, flow_buffers(A.mode) * BUF, h->stream>>>(A);
+    } else {
+      auto k = flow_kernel<TH, R, TX, TY, NT, false>;
+      set_smem(k, BUF, smem_done_flow);
+      k<<<h->nblocks, NT, BUF, h->stream>>>(A);
+    }
     CK(cudaGetLastError());
     return SS_OK;
   }
@@ -275,9 +319,16 @@ struct Fused {
     FlowArgs<R> A = base_args(h);
     A.E_traj = E_dev;
     A.err_traj = err_dev;
+    const bool tma = h->tma;
+    // maps: [0] field [1] velocity [2] phi_alt [3] vel_alt [4] l1 [5] l2
+    int cur = 0;
     for (int s = 0; s < n; ++s) {
       A.phi = cur_p;
       A.vel = cur_v;
+      if (tma) {
+        A.tm_phi = h->tm[cur == 0 ? 0 : 2];
+        A.tm_vel = h->tm[cur == 0 ? 1 : 3];
+      }
       // S1: l1 = -dt G(phi); energy of phi (the previous step's result) + arrest test
       A.mode = M_S1;
       A.out_l = l1;
@@ -286,7 +337,7 @@ struct Fused {
       A.E_idx = s - 1;
       A.init_state = s == 0;
       A.prev_energy = prev;
-      int rc = launch(h, A);
+      int rc = launch(h, A, tma);
       if (rc) return rc;
       A.with_energy = 0;
       A.arrest_update = 0;
@@ -295,11 +346,12 @@ struct Fused {
       // S2, S3
       A.mode = M_S2;
       A.out_l = l2;
-      if ((rc = launch(h, A))) return rc;
+      if ((rc = launch(h, A, tma))) return rc;
       A.mode = M_S3;
       A.la = l1;
       A.out_l = l3;
-      if ((rc = launch(h, A))) return rc;
+      if (tma) A.tm_l = h->tm[4];
+      if ((rc = launch(h, A, tma))) return rc;
       // S4 + finalize into the ping-pong buffers
       A.mode = M_S4;
       A.la = l1;
@@ -309,10 +361,12 @@ struct Fused {
       A.phi_out = alt_p;
       A.vel_out = alt_v;
       A.err_idx = s;
-      if ((rc = launch(h, A))) return rc;
+      if (tma) A.tm_l = h->tm[5];
+      if ((rc = launch(h, A, tma))) return rc;
       A.err_idx = -1;
       std::swap(cur_p, alt_p);
       std::swap(cur_v, alt_v);
+      cur ^= 1;
     }
     // trailing energy of the final field + arrest test
     A.phi = cur_p;
@@ -320,7 +374,8 @@ struct Fused {
     A.with_energy = 1;
     A.arrest_update = 1;
     A.E_idx = n - 1;
-    int rc = launch(h, A);
+    if (tma) A.tm_phi = h->tm[cur == 0 ? 0 : 2];
+    int rc = launch(h, A, tma);
     if (rc) return rc;
     const long long nfN = (long long)h->nf * h->G.N;
     finish_kernel<R><<<grid_1d(nfN), 256, 0, h->stream>>>(cur_p, cur_v, field, vel, nfN, cur_p != field ? 1 : 0,
@@ -335,7 +390,8 @@ struct Fused {
     A.phi = (const R*)field;
     A.out_eg = (R*)eg;
     A.out_l = (R*)l_out;
-    return launch(h, A);
+    const bool tma = encode_tile_map(&A.tm_phi, field, sizeof(R), h->G.X, h->G.Y, TH::NF);
+    return launch(h, A, tma);
   }
 
   static int energy(ss_handle* h, const void* field) {
@@ -343,13 +399,14 @@ struct Fused {
     A.mode = M_ENERGY;
     A.phi = (const R*)field;
     A.with_energy = 1;
-    return launch(h, A);
+    const bool tma = encode_tile_map(&A.tm_phi, field, sizeof(R), h->G.X, h->G.Y, TH::NF);
+    return launch(h, A, tma);
   }
 
   static int density(ss_handle* h, const void* field, double* dens, bool reduce, int kind, int which) {
     auto k = density_kernel<TH, R, TX, TY, NT>;
-    set_smem(k, SMEM, smem_done_density);
-    k<<<h->nblocks, NT, SMEM, h->stream>>>((const R*)field, dens, reduce ? h->partial : nullptr, h->st, kind, which,
+    set_smem(k, BUF, smem_done_density);
+    k<<<h->nblocks, NT, BUF, h->stream>>>((const R*)field, dens, reduce ? h->partial : nullptr, h->st, kind, which,
                                            h->G, h->P);
     CK(cudaGetLastError());
     return SS_OK;
@@ -484,6 +541,8 @@ int take_status(ss_handle* h) {
     const int zero = 0;
     CK(cudaMemcpyAsync(&h->st->status, &zero, sizeof(int), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    if (s.status == SS_ERR_TIMEOUT)
+      return fail(SS_ERR_TIMEOUT, "a device-side wait timed out; re-bind the handle before further use");
     return fail(SS_ERR_NONFINITE, "a reduction produced a non-finite value");
   }
   return SS_OK;
@@ -543,6 +602,7 @@ const char* ss_status_string(int status) {
     case SS_ERR_NONFINITE: return "non-finite value";
     case SS_ERR_STATE: return "invalid call order";
     case SS_ERR_WORKSPACE: return "workspace too small or misaligned";
+    case SS_ERR_TIMEOUT: return "device-side wait timed out";
   }
   return "unknown status";
 }
@@ -606,8 +666,17 @@ int ss_bind(ss_handle* h, void* field, void* velocity, void* workspace, size_t w
   CK(cudaMemcpyAsync(h->st, &init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->E_last_host = NAN;
+  h->tma = false;
+  if (h->precision != SS_PLAIN_FP64 && field && velocity) {
+    const void* bufs[6] = {field, velocity, h->phi_alt, h->vel_alt, h->l[0], h->l[1]};
+    bool ok = true;
+    for (int i = 0; i < 6 && ok; ++i) ok = encode_tile_map(&h->tm[i], bufs[i], h->elem, h->G.X, h->G.Y, h->nf);
+    h->tma = ok;
+  }
   return SS_OK;
 }
+
+int ss_tma_enabled(const ss_handle* h) { return h && h->tma ? 1 : 0; }
 
 int ss_step_async(ss_handle* h, int n_steps, double prev_energy, double* energy_traj_dev, double* err_traj_dev) {
   int rc = check_bound(h);

@@ -104,24 +104,18 @@ struct FD {
   static constexpr double c52 = 5.0 / 2.0;
 };
 
-// First derivative from the 4 stencil values.  FP64 keeps the reference's
-// association; FP32 uses the difference form: for a smooth field f(+k) - f(-k) is
-// exact (Sterbenz), so the rounding error scales with the derivative, not with |f|.
+// First and second derivatives from the 5-point stencil values, in difference
+// form: for a smooth field f(+k) - f(-k) and f(+k) - f(0) are exact (Sterbenz), so
+// the rounding error scales with the derivative rather than with |f|, and a
+// constant field has exactly zero derivatives.  (The reference's association,
+// derivatives.py:51-110, leaves O(eps |f| / h) residues; the two agree to that level.)
 template <typename R>
 __device__ inline R d1_stencil(R m2, R m1, R p1, R p2, R inv_h) {
-  if constexpr (sizeof(R) == 8) {
-    return (FD::c12 * m2 - FD::c23 * m1 + FD::c23 * p1 - FD::c12 * p2) * inv_h;
-  } else {
-    return ((R)FD::c23 * (p1 - m1) - (R)FD::c12 * (p2 - m2)) * inv_h;
-  }
+  return ((R)FD::c23 * (p1 - m1) - (R)FD::c12 * (p2 - m2)) * inv_h;
 }
 template <typename R>
 __device__ inline R d2_stencil(R m2, R m1, R c, R p1, R p2, R inv_h2) {
-  if constexpr (sizeof(R) == 8) {
-    return (-FD::c12 * m2 + FD::c43 * m1 - FD::c52 * c + FD::c43 * p1 - FD::c12 * p2) * inv_h2;
-  } else {
-    return ((R)FD::c43 * ((p1 - c) + (m1 - c)) - (R)FD::c12 * ((p2 - c) + (m2 - c))) * inv_h2;
-  }
+  return ((R)FD::c43 * ((p1 - c) + (m1 - c)) - (R)FD::c12 * ((p2 - c) + (m2 - c))) * inv_h2;
 }
 
 // Inverse spacings in the working precision.

@@ -19,15 +19,26 @@
 // closes a call.  Compulsory traffic: 16 words per site and step.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 #include "theories.cuh"
 
 namespace ssb {
 
 enum FlowMode { M_GRAD = 0, M_S1 = 1, M_S2 = 2, M_S3 = 3, M_S4 = 4, M_ENERGY = 5 };
+enum { ST_TIMEOUT = 6 };
+
+// Upper bound of a device-side wait on an mbarrier (~1 s at 1.9 GHz).  On expiry
+// the kernel records ST_TIMEOUT, waits the same bound again for its copies in
+// flight and returns without computing.
+constexpr long long WAIT_CYCLES = 2000000000LL;
 
 template <typename R>
 struct FlowArgs {
+  CUtensorMap tm_phi;  // TMA maps (used when the kernel is instantiated with TMA)
+  CUtensorMap tm_vel;
+  CUtensorMap tm_l;    // l1 (S3) or l2 (S4)
   const R* phi;
   const R* vel;
   const R* la;  // l1 (S3, S4)
@@ -52,66 +63,131 @@ struct FlowArgs {
   Phys P;
 };
 
+// Tile of TX x TY sites.  Staged planes hold rows x0-2 .. x0+TX+1 and columns
+// y0-4 .. y0+TY+3: the y start is rounded down to a 16-byte boundary so the same
+// geometry serves TMA boxes and plain loads; the stencil uses columns 2 .. TY+5.
 template <int TX, int TY, int NT>
 struct TileShape {
-  static constexpr int HX = TX + 4, HY = TY + 4;
+  static constexpr int HX = TX + 4, HY = TY + 8, YOFF = 4;
+  static constexpr int PLANE = HX * HY;
   static constexpr int ROWS_PER_PASS = NT / TY;
   static constexpr int SITES_PER_THREAD = TX / ROWS_PER_PASS;
   static_assert(NT % TY == 0 && TX % (NT / TY) == 0, "tile/thread mismatch");
+  static_assert(TY % 4 == 0, "TY must keep the y start 16-byte aligned");
 };
 
 template <typename R, int NF, int TX, int TY>
-__host__ __device__ constexpr size_t tile_bytes() {
-  return sizeof(R) * NF * (TX + 4) * (TY + 4);
+__host__ __device__ constexpr size_t tile_buf_bytes() {
+  return sizeof(R) * NF * (TX + 4) * (TY + 8);
 }
 
-// Stage the (TX+4) x (TY+4) halo tile of T_s (formed on the fly from phi, V, l) into
-// shared memory.  Out-of-lattice entries are 0 and never enter a masked derivative.
+// number of staged buffers a mode needs (phi, then velocity, then l)
+__host__ __device__ inline int flow_buffers(int mode) {
+  return mode == M_S2 ? 2 : (mode == M_S3 || mode == M_S4) ? 3 : 1;
+}
+
+// ---------------------------------------------------------------------------
+// TMA / mbarrier helpers (inline PTX, sm_90+ instructions, used on sm_100a)
+// ---------------------------------------------------------------------------
+__device__ inline uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ inline void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ inline bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// 3-D tiled bulk tensor load global -> shared (no multicast), completion on `bar`.
+__device__ inline void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+// Bounded wait; returns false when WAIT_CYCLES elapsed first.
+__device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > WAIT_CYCLES) return false;
+  }
+  return true;
+}
+
+// T_s for one element from the staged inputs (the reference's k / Temp algebra,
+// core/integrator.py:51-96 and :323-334)
+template <typename R>
+__device__ inline R stage_value(int mode, R p, R v, R w, R dt) {
+  const R half = (R)0.5;
+  if (mode == M_S2) return p + half * (dt * v);
+  if (mode == M_S3) return p + half * (dt * (v + half * w));
+  if (mode == M_S4) return p + dt * (v + half * w);
+  return p;
+}
+
+// Plain-load staging of T_s into `T` (all components), used when a TMA map cannot
+// describe the buffers (row pitch not a multiple of 16 bytes).  Every thread first
+// issues all loads of one component plane, then combines and stores, so each
+// plane costs one memory round trip.
 template <int NF, typename R, int TX, int TY, int NT>
-__device__ inline void stage_tile(R* tile, const FlowArgs<R>& A, int x0, int y0, int mode, bool arrest) {
+__device__ inline void stage_plain(R* T, const FlowArgs<R>& A, int x0, int y0, int mode, bool arrest) {
   using TS = TileShape<TX, TY, NT>;
+  constexpr int KM = (TS::PLANE + NT - 1) / NT;
   const Grid& G = A.G;
   const long long N = G.N;
   const R dt = (R)G.dt;
-  const R half = (R)0.5;
+  long long off[KM];
+  bool ok[KM];
+#pragma unroll
+  for (int k = 0; k < KM; ++k) {
+    const int i = threadIdx.x + k * NT;
+    const int r = i / TS::HY, c = i - r * TS::HY;
+    const int gx = x0 - 2 + r, gy = y0 - TS::YOFF + c;
+    ok[k] = i < TS::PLANE && gx >= 0 && gx < G.X && gy >= 0 && gy < G.Y;
+    off[k] = (long long)gx * G.Y + gy;
+  }
+  const bool need_v = (mode == M_S2 || mode == M_S3 || mode == M_S4) && !arrest;
+  const R* lsrc = mode == M_S3 ? A.la : (mode == M_S4 ? A.lb : nullptr);
 #pragma unroll
   for (int a = 0; a < NF; ++a) {
-    for (int i = threadIdx.x; i < TS::HX * TS::HY; i += NT) {
-      const int r = i / TS::HY, c = i - r * TS::HY;
-      const int gx = x0 - 2 + r, gy = y0 - 2 + c;
-      R t = (R)0;
-      if (gx >= 0 && gx < G.X && gy >= 0 && gy < G.Y) {
-        const long long idx = (long long)a * N + (long long)gx * G.Y + gy;
-        const R p = A.phi[idx];
-        if (mode == M_S2) {
-          const R v = arrest ? (R)0 : A.vel[idx];
-          t = p + half * (dt * v);
-        } else if (mode == M_S3) {
-          const R v = arrest ? (R)0 : A.vel[idx];
-          const R w = A.la[idx];
-          t = p + half * (dt * (v + half * w));
-        } else if (mode == M_S4) {
-          const R v = arrest ? (R)0 : A.vel[idx];
-          const R w = A.lb[idx];
-          t = p + dt * (v + half * w);
-        } else {
-          t = p;
-        }
-      }
-      tile[(a * TS::HX + r) * TS::HY + c] = t;
+    R p[KM], v[KM], w[KM];
+    const long long base = (long long)a * N;
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+      p[k] = ok[k] ? A.phi[base + off[k]] : (R)0;
+      v[k] = (ok[k] && need_v) ? A.vel[base + off[k]] : (R)0;
+      w[k] = (ok[k] && lsrc) ? lsrc[base + off[k]] : (R)0;
+    }
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+      const int i = threadIdx.x + k * NT;
+      if (i < TS::PLANE) T[a * TS::PLANE + i] = stage_value<R>(mode, p[k], v[k], w[k], dt);
     }
   }
 }
 
-template <class TH, typename R, int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) flow_kernel(const FlowArgs<R> A) {
+template <class TH, typename R, int TX, int TY, int NT, bool TMA>
+__global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowArgs<R> A) {
   using TS = TileShape<TX, TY, NT>;
   constexpr int NF = TH::NF;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* tile = reinterpret_cast<R*>(smem_raw);
+  constexpr int BUF = NF * TS::PLANE;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  R* B0 = reinterpret_cast<R*>(smem_raw);
+  R* B1 = B0 + BUF;
+  R* B2 = B1 + BUF;
   __shared__ double red[NT / 32];
   __shared__ double sh_s[NT], sh_c[NT];
   __shared__ int am_last;
+  __shared__ __align__(8) uint64_t bar;
 
   const Grid& G = A.G;
   const int mode = A.mode;
@@ -122,18 +198,53 @@ __global__ void __launch_bounds__(NT) flow_kernel(const FlowArgs<R> A) {
   StepState* st = A.st;
   const bool arrest = (mode == M_S2 || mode == M_S3 || mode == M_S4) && (st->arrest != 0);
   const bool do_energy = A.with_energy != 0;
+  const R dt = (R)G.dt;
 
   if (A.init_state && blockIdx.x == 0 && threadIdx.x == 0) {
     st->arrest = 0;
     if (!isnan(A.prev_energy)) st->E_last = A.prev_energy;
   }
 
-  stage_tile<NF, R, TX, TY, NT>(tile, A, x0, y0, mode, arrest);
-  __syncthreads();
+  // ---- stage the halo tile of T_s --------------------------------------
+  R* T = B0;
+  if constexpr (TMA) {
+    const bool need_v = (mode == M_S2 || mode == M_S3 || mode == M_S4) && !arrest;
+    const bool need_l = mode == M_S3 || mode == M_S4;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t bytes = (uint32_t)(sizeof(R) * BUF) * (1u + (need_v ? 1u : 0u) + (need_l ? 1u : 0u));
+      mbar_expect_tx(&bar, bytes);
+      tma_load_3d(B0, &A.tm_phi, y0 - TS::YOFF, x0 - 2, 0, &bar);
+      if (need_v) tma_load_3d(B1, &A.tm_vel, y0 - TS::YOFF, x0 - 2, 0, &bar);
+      if (need_l) tma_load_3d(B2, &A.tm_l, y0 - TS::YOFF, x0 - 2, 0, &bar);
+    }
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0));
+    if (!ok) {
+      if (threadIdx.x == 0) atomicExch(&st->status, (int)ST_TIMEOUT);
+      mbar_wait_bounded(&bar, 0);
+      return;
+    }
+    if (mode == M_S2 || mode == M_S3 || mode == M_S4) {
+      // combine in place into the last staged buffer (OOB entries are zero in all)
+      R* dst = need_l ? B2 : (need_v ? B1 : B0);
+      if (dst != B0) {
+        for (int i = threadIdx.x; i < BUF; i += NT) {
+          const R v = need_v ? B1[i] : (R)0;
+          const R w = need_l ? B2[i] : (R)0;
+          dst[i] = stage_value<R>(mode, B0[i], v, w, dt);
+        }
+        __syncthreads();
+      }
+      T = dst;
+    }
+  } else {
+    stage_plain<NF, R, TX, TY, NT>(B0, A, x0, y0, mode, arrest);
+    __syncthreads();
+  }
 
   const Inv<R> iv(G);
   const Inv<double> ivd(G);
-  const R dt = (R)G.dt;
   const int ly = threadIdx.x % TY;
   const int lxg = threadIdx.x / TY;
   double e_acc = 0.0;
@@ -145,13 +256,13 @@ __global__ void __launch_bounds__(NT) flow_kernel(const FlowArgs<R> A) {
     const int gx = x0 + lx, gy = y0 + ly;
     if (gx >= G.X || gy >= G.Y) continue;
     const Masks mk = site_masks(G, gx, gy);
-    const R* base = tile + (lx + 2) * TS::HY + (ly + 2);
+    const R* base = T + (lx + 2) * TS::HY + (ly + TS::YOFF);
 
     if (do_energy) {
       Jet1<double, NF> J1;
 #pragma unroll
       for (int a = 0; a < NF; ++a) {
-        const R* pa = base + a * TS::HX * TS::HY;
+        const R* pa = base + a * TS::PLANE;
         auto acc = [pa](int dx, int dy) -> double { return (double)pa[dx * TS::HY + dy]; };
         fill_jet1_comp<double>(acc, mk, ivd, J1.f[a], J1.dx[a], J1.dy[a]);
       }
@@ -162,7 +273,7 @@ __global__ void __launch_bounds__(NT) flow_kernel(const FlowArgs<R> A) {
     Jet<R, NF> J;
 #pragma unroll
     for (int a = 0; a < NF; ++a) {
-      const R* pa = base + a * TS::HX * TS::HY;
+      const R* pa = base + a * TS::PLANE;
       auto acc = [pa](int dx, int dy) -> R { return pa[dx * TS::HY + dy]; };
       fill_jet_comp<R>(acc, mk, iv, J.f[a], J.dx[a], J.dy[a], J.dxx[a], J.dyy[a], J.dxy[a], TH::NEED_XY);
     }
@@ -296,7 +407,7 @@ __global__ void __launch_bounds__(NT)
                    int which, Grid G, Phys P) {
   using TS = TileShape<TX, TY, NT>;
   constexpr int NF = TH::NF;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   R* tile = reinterpret_cast<R*>(smem_raw);
   __shared__ double red[NT / 32];
   __shared__ double sh_s[NT], sh_c[NT];
@@ -304,16 +415,11 @@ __global__ void __launch_bounds__(NT)
   const int tiles_y = (G.Y + TY - 1) / TY;
   const int x0 = (blockIdx.x / tiles_y) * TX;
   const int y0 = (blockIdx.x % tiles_y) * TY;
-  const long long N = G.N;
-#pragma unroll
-  for (int a = 0; a < NF; ++a) {
-    for (int i = threadIdx.x; i < TS::HX * TS::HY; i += NT) {
-      const int r = i / TS::HY, c = i - r * TS::HY;
-      const int gx = x0 - 2 + r, gy = y0 - 2 + c;
-      R t = (R)0;
-      if (gx >= 0 && gx < G.X && gy >= 0 && gy < G.Y) t = phi[(long long)a * N + (long long)gx * G.Y + gy];
-      tile[(a * TS::HX + r) * TS::HY + c] = t;
-    }
+  {
+    FlowArgs<R> A;
+    A.phi = phi;
+    A.G = G;
+    stage_plain<NF, R, TX, TY, NT>(tile, A, x0, y0, M_GRAD, false);
   }
   __syncthreads();
   const Inv<double> ivd(G);
@@ -326,11 +432,11 @@ __global__ void __launch_bounds__(NT)
     const int gx = x0 + lx, gy = y0 + ly;
     if (gx >= G.X || gy >= G.Y) continue;
     const Masks mk = site_masks(G, gx, gy);
-    const R* base = tile + (lx + 2) * TS::HY + (ly + 2);
+    const R* base = tile + (lx + 2) * TS::HY + (ly + TS::YOFF);
     Jet1<double, NF> J1;
 #pragma unroll
     for (int a = 0; a < NF; ++a) {
-      const R* pa = base + a * TS::HX * TS::HY;
+      const R* pa = base + a * TS::PLANE;
       auto accs = [pa](int dx, int dy) -> double { return (double)pa[dx * TS::HY + dy]; };
       fill_jet1_comp<double>(accs, mk, ivd, J1.f[a], J1.dx[a], J1.dy[a]);
     }
