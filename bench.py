@@ -206,6 +206,7 @@ def gpu_arm(args, rank, world, local_rank):
     E_traj = torch.empty(K, dtype=torch.float64, device=dev)
     err_traj = torch.empty(K, dtype=torch.float64, device=dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tuning = s.autotune(5)
     with Clocks(local_rank) as clk:
         # warm-up (untimed); also gives the clock sampler time to start
         s.step(max(W, 1), 1e300)
@@ -285,7 +286,9 @@ def gpu_arm(args, rank, world, local_rank):
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": Ke, "api": "Simulation.step(prev_energy) per step"},
-                "gpu_launches": launches, "clocks": clk.summary()}
+                "gpu_launches": launches, "clocks": clk.summary(),
+                "autotune": {f"S{m}": {"tile_per_cta_ms": a, "pipelined_ms": b, "chosen": "pipelined" if c else
+                                       "tile_per_cta"} for m, (a, b, c) in tuning.items()}}
         line.update(extra)
         print(json.dumps(line), flush=True)
     return 0

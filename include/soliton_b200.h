@@ -108,6 +108,13 @@ int ss_check_status(ss_handle *h);
 /* 1 when the bound Field/Velocity/workspace buffers are staged by TMA tensor maps
  * (row pitch and base 16-byte aligned), 0 when the plain-load path is used. */
 int ss_tma_enabled(const ss_handle *h);
+/* Autotuner: times, on the bound buffers, the two TMA staging variants of each flow
+ * stage (a persistent CTA per SM walking tiles through a shared-memory ring, or one
+ * tile per CTA) over `iters` launches and keeps the faster one.  Writes only
+ * workspace scratch.  ms_out (nullable, 12 floats) receives [mode][variant] times. */
+int ss_autotune(ss_handle *h, int iters, float *ms_out);
+/* Variant chosen for a flow mode (0..5): 1 pipelined, 0 one tile per CTA, -1 bad args. */
+int ss_get_variant(const ss_handle *h, int mode);
 
 /* One gradient evaluation of an arbitrary field buffer: energy_gradient (nullable)
  * receives the theory's projected dE/dphi, l_out (nullable) receives -dt*dE/dphi.

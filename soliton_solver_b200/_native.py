@@ -75,6 +75,8 @@ _SIG = {
     "ss_step_async": ([_P, _I, _D, _P, _P], _I),
     "ss_check_status": ([_P], _I),
     "ss_tma_enabled": ([_P], _I),
+    "ss_autotune": ([_P, _I, _P], _I),
+    "ss_get_variant": ([_P, _I], _I),
     "ss_gradient": ([_P, _P, _P, _P], _I),
     "ss_energy_density": ([_P, _P, _P], _I),
     "ss_energy": ([_P, _P, ctypes.POINTER(_D)], _I),

@@ -120,6 +120,16 @@ class Solver:
         """True when the bound buffers are staged with TMA tensor maps."""
         return bool(self._lib.ss_tma_enabled(self._h))
 
+    def autotune(self, iters: int = 5):
+        """Pick the faster TMA staging variant of each flow stage on the bound buffers.
+
+        Returns {stage: (ms one-tile-per-CTA, ms pipelined, chosen)} for stages 1-4."""
+        ms = np.zeros(12, dtype=np.float32)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_autotune(self._h, int(iters), ms.ctypes.data))
+        return {m: (float(ms[2 * m]), float(ms[2 * m + 1]), int(self._lib.ss_get_variant(self._h, m)))
+                for m in (1, 2, 3, 4)}
+
     def check_status(self):
         nat.check(self._lib.ss_check_status(self._h))
 

@@ -60,13 +60,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // 3-D map over component planes (dims y, x, component) whose box is one staged
 // tile: (TY + 8) x (TX + 4) x NF.  Fails (-> plain loads) when the buffer or its
 // row pitch is not 16-byte aligned.
-bool encode_tile_map(CUtensorMap* m, const void* ptr, size_t es, int X, int Y, int NF) {
+bool encode_tile_map(CUtensorMap* m, const void* ptr, size_t es, int X, int Y, int NF, bool centre = false) {
   if (!ptr || ((uintptr_t)ptr) % 16 || ((size_t)Y * es) % 16) return false;
   auto fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[3] = {(cuuint64_t)Y, (cuuint64_t)X, (cuuint64_t)NF};
   cuuint64_t strides[2] = {(cuuint64_t)Y * es, (cuuint64_t)X * Y * es};
-  cuuint32_t box[3] = {(cuuint32_t)(TY + 8), (cuuint32_t)(TX + 4), (cuuint32_t)NF};
+  cuuint32_t box[3] = {(cuuint32_t)(centre ? TY : TY + 8), (cuuint32_t)(centre ? TX : TX + 4), (cuuint32_t)NF};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(m, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
                   const_cast<void*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -107,9 +107,14 @@ struct ss_handle {
   double* entmp = nullptr;
   double E_last_host = NAN;
   std::vector<double> host_partial;
-  // TMA maps of the bound buffers: field, velocity, phi_alt, vel_alt, l1, l2
-  CUtensorMap tm[6];
+  // TMA maps of the bound buffers: field, velocity, phi_alt, vel_alt, l1, l2 (halo
+  // boxes), then l1 and l3 centre boxes
+  CUtensorMap tm[8];
   bool tma = false;
+  int num_sms = 148;
+  // per flow mode: 1 = persistent pipelined kernel, 0 = one tile per CTA (autotuned)
+  int use_pipe[6] = {1, 1, 1, 1, 1, 1};
+  float tune_ms[6][2] = {};
 };
 
 namespace {
@@ -188,6 +193,17 @@ int decode(ss_handle* h, int theory, const int32_t* p_i, int n_i, const double* 
       !std::isfinite(G.dt))
     return fail(SS_ERR_ARG, "lattice spacings / time step must be finite and positive");
   h->nf = nf;
+  {
+    const double c12 = 1.0 / 12.0, c23 = 2.0 / 3.0, c43 = 4.0 / 3.0;
+    double* k = G.kd;
+    k[GK_C23HX] = c23 * G.ihx;   k[GK_MC12HX] = -c12 * G.ihx;
+    k[GK_C43HX2] = c43 * G.ihx2; k[GK_MC12HX2] = -c12 * G.ihx2;
+    k[GK_C23HY] = c23 * G.ihy;   k[GK_MC12HY] = -c12 * G.ihy;
+    k[GK_C43HY2] = c43 * G.ihy2; k[GK_MC12HY2] = -c12 * G.ihy2;
+    k[GK_C43HD] = c43 * G.ih2dA; k[GK_MC12HD] = -c12 * G.ih2dA;
+    k[GK_DT] = G.dt; k[GK_MDT] = -G.dt; k[GK_HDT] = 0.5 * G.dt; k[GK_DT6] = G.dt / 6.0; k[GK_SIXTH] = 1.0 / 6.0;
+    for (int i = 0; i < 16; ++i) G.kf[i] = (float)G.kd[i];
+  }
   Phys& P = h->P;
   memset(&P, 0, sizeof(P));
   switch (theory) {
@@ -240,6 +256,13 @@ int decode(ss_handle* h, int theory, const int32_t* p_i, int n_i, const double* 
       break;
     }
   }
+  switch (theory) {
+    case SS_THEORY_CHIRAL_MAGNET: ChiralMagnet::derive(P); break;
+    case SS_THEORY_BABY_SKYRME: BabySkyrme::derive(P); break;
+    case SS_THEORY_GINZBURG_LANDAU: GinzburgLandau::derive(P); break;
+    case SS_THEORY_ANISOTROPIC: Anisotropic::derive(P); break;
+  }
+  for (int i = 0; i < 24; ++i) P.cf[i] = (float)P.c[i];
   return SS_OK;
 }
 
@@ -274,21 +297,99 @@ dim3 grid_1d(long long n) {
 template <class TH, typename R>
 struct Fused {
   static constexpr size_t BUF = tile_buf_bytes<R, TH::NF, TX, TY>();
-  static inline unsigned long long smem_done_flow = 0, smem_done_tma = 0, smem_done_density = 0;
+  static inline unsigned long long smem_done_density = 0;
 
   // tma: use the TMA-staged instantiation (A.tm_* must describe A's buffers)
-  static int launch(const ss_handle* h, const FlowArgs<R>& A, bool tma) {
-    if (tma) {
-      auto k = flow_kernel<TH, R, TX, TY, NT, true>;
-      set_smem(k, 3 * BUF, smem_done_tma);
-      k<<<h->nblocks, NT, flow_buffers(A.mode) * BUF, h->stream>>>(A);
-    } else {
-      auto k = flow_kernel<TH, R, TX, TY, NT, false>;
-      set_smem(k, BUF, smem_done_flow);
-      k<<<h->nblocks, NT, BUF, h->stream>>>(A);
-    }
+  static inline unsigned long long smem_done[2][6] = {};
+
+  // dynamic shared memory of flow_kernel: the staged buffers, plus (FP32 energy
+  // stages) room for the FP64 copy of the tile after the first buffer
+  template <bool TMA_, int MODE>
+  static constexpr size_t flow_smem() {
+    const size_t staged = TMA_ ? flow_buffers(MODE) * BUF : BUF;
+    const size_t energy = (sizeof(R) == 4 && (MODE == M_S1 || MODE == M_ENERGY)) ? BUF + 2 * BUF : 0;
+    return staged > energy ? staged : energy;
+  }
+
+  template <bool TMA_, int MODE>
+  static int launch_mode(const ss_handle* h, const FlowArgs<R>& A) {
+    auto k = flow_kernel<TH, R, TX, TY, NT, TMA_, MODE>;
+    const size_t smem = flow_smem<TMA_, MODE>();
+    set_smem(k, smem, smem_done[TMA_ ? 1 : 0][MODE]);
+    k<<<h->nblocks, NT, smem, h->stream>>>(A);
     CK(cudaGetLastError());
     return SS_OK;
+  }
+
+  template <bool TMA_>
+  static int launch_tma(const ss_handle* h, const FlowArgs<R>& A) {
+    switch (A.mode) {
+      case M_GRAD: return launch_mode<TMA_, M_GRAD>(h, A);
+      case M_S1: return launch_mode<TMA_, M_S1>(h, A);
+      case M_S2: return launch_mode<TMA_, M_S2>(h, A);
+      case M_S3: return launch_mode<TMA_, M_S3>(h, A);
+      case M_S4: return launch_mode<TMA_, M_S4>(h, A);
+      case M_ENERGY: return launch_mode<TMA_, M_ENERGY>(h, A);
+    }
+    return fail(SS_ERR_ARG, "bad flow mode");
+  }
+
+  // persistent TMA-pipelined variant: FP32 fields and at least two ring slots
+  static constexpr int PIPE_NT = 512;
+  template <int MODE>
+  static constexpr int pipe_stages() {
+    const size_t slot = pipe_slot_bytes<R, TH::NF, TX, TY, MODE>();
+    const size_t budget = 212 * 1024;  // dynamic shared memory left next to the static reduction arrays
+    const int n = (int)(budget / slot);
+    return n > 4 ? 4 : n;
+  }
+  template <int MODE>
+  static constexpr bool pipe_ok() {
+    return sizeof(R) == 4 && pipe_stages<MODE>() >= 2;
+  }
+  static inline unsigned long long smem_done_pipe[6] = {};
+
+  template <int MODE>
+  static int launch_pipe(const ss_handle* h, const FlowArgs<R>& A) {
+    if constexpr (pipe_ok<MODE>()) {
+      constexpr int S = pipe_stages<MODE>();
+      auto k = flow_kernel_pipe<TH, R, TX, TY, PIPE_NT, MODE, S>;
+      const size_t smem = S * pipe_slot_bytes<R, TH::NF, TX, TY, MODE>();
+      set_smem(k, smem, smem_done_pipe[MODE]);
+      const int grid = std::min(h->nblocks, h->num_sms);
+      k<<<grid, PIPE_NT, smem, h->stream>>>(A);
+      CK(cudaGetLastError());
+      return SS_OK;
+    } else {
+      return launch_mode<true, MODE>(h, A);
+    }
+  }
+
+  static bool uses_pipe(int mode) {
+    switch (mode) {
+      case M_GRAD: return pipe_ok<M_GRAD>();
+      case M_S1: return pipe_ok<M_S1>();
+      case M_S2: return pipe_ok<M_S2>();
+      case M_S3: return pipe_ok<M_S3>();
+      case M_S4: return pipe_ok<M_S4>();
+      case M_ENERGY: return pipe_ok<M_ENERGY>();
+    }
+    return false;
+  }
+
+  // tma: use the TMA-staged instantiations (A.tm_* must describe A's buffers)
+  static int launch(const ss_handle* h, const FlowArgs<R>& A, bool tma) {
+    if (!tma) return launch_tma<false>(h, A);
+    if (!h->use_pipe[A.mode]) return launch_tma<true>(h, A);
+    switch (A.mode) {
+      case M_GRAD: return launch_pipe<M_GRAD>(h, A);
+      case M_S1: return launch_pipe<M_S1>(h, A);
+      case M_S2: return launch_pipe<M_S2>(h, A);
+      case M_S3: return launch_pipe<M_S3>(h, A);
+      case M_S4: return launch_pipe<M_S4>(h, A);
+      case M_ENERGY: return launch_pipe<M_ENERGY>(h, A);
+    }
+    return fail(SS_ERR_ARG, "bad flow mode");
   }
 
   static FlowArgs<R> base_args(const ss_handle* h) {
@@ -361,7 +462,11 @@ struct Fused {
       A.phi_out = alt_p;
       A.vel_out = alt_v;
       A.err_idx = s;
-      if (tma) A.tm_l = h->tm[5];
+      if (tma) {
+        A.tm_l = h->tm[5];
+        A.tm_c1 = h->tm[6];
+        A.tm_c3 = h->tm[7];
+      }
       if ((rc = launch(h, A, tma))) return rc;
       A.err_idx = -1;
       std::swap(cur_p, alt_p);
@@ -382,6 +487,59 @@ struct Fused {
                                                           h->st);
     CK(cudaGetLastError());
     return SS_OK;
+  }
+
+  // Time both staging variants of every stage on the bound buffers (writes only
+  // workspace scratch: l1..l3 and the ping-pong copies) and keep the faster one.
+  static int autotune(ss_handle* h, int iters) {
+    if (!h->tma) return SS_OK;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    FlowArgs<R> A = base_args(h);
+    A.phi = (const R*)h->field;
+    A.vel = (const R*)h->vel;
+    A.la = (const R*)h->l[0];
+    A.lb = (const R*)h->l[1];
+    A.lc = (const R*)h->l[2];
+    A.phi_out = (R*)h->phi_alt;
+    A.vel_out = (R*)h->vel_alt;
+    A.tm_phi = h->tm[0];
+    A.tm_vel = h->tm[1];
+    A.tm_c1 = h->tm[6];
+    A.tm_c3 = h->tm[7];
+    const int modes[4] = {M_S1, M_S2, M_S3, M_S4};
+    int rc = SS_OK;
+    for (int mi = 0; mi < 4 && rc == SS_OK; ++mi) {
+      const int m = modes[mi];
+      A.mode = m;
+      A.out_l = m == M_S1 ? (R*)h->l[0] : m == M_S2 ? (R*)h->l[1] : m == M_S3 ? (R*)h->l[2] : nullptr;
+      A.tm_l = m == M_S3 ? h->tm[4] : h->tm[5];
+      A.with_energy = m == M_S1 ? 1 : 0;
+      if (!uses_pipe(m)) {
+        h->use_pipe[m] = 0;
+        continue;
+      }
+      for (int v = 0; v < 2 && rc == SS_OK; ++v) {
+        h->use_pipe[m] = v;
+        rc = launch(h, A, true);  // warm-up
+        if (rc) break;
+        CK(cudaEventRecord(e0, h->stream));
+        for (int i = 0; i < iters && rc == SS_OK; ++i) rc = launch(h, A, true);
+        CK(cudaEventRecord(e1, h->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        h->tune_ms[m][v] = ms / iters;
+      }
+      h->use_pipe[m] = h->tune_ms[m][1] <= h->tune_ms[m][0] ? 1 : 0;
+    }
+    // the energy-only pass must reduce exactly like stage 1 (same grid and tile order)
+    h->use_pipe[M_ENERGY] = h->use_pipe[M_S1];
+    h->use_pipe[M_GRAD] = h->use_pipe[M_S2];
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
   }
 
   static int gradient(ss_handle* h, const void* field, void* eg, void* l_out) {
@@ -668,15 +826,45 @@ int ss_bind(ss_handle* h, void* field, void* velocity, void* workspace, size_t w
   h->E_last_host = NAN;
   h->tma = false;
   if (h->precision != SS_PLAIN_FP64 && field && velocity) {
-    const void* bufs[6] = {field, velocity, h->phi_alt, h->vel_alt, h->l[0], h->l[1]};
+    const void* bufs[8] = {field, velocity, h->phi_alt, h->vel_alt, h->l[0], h->l[1], h->l[0], h->l[2]};
     bool ok = true;
-    for (int i = 0; i < 6 && ok; ++i) ok = encode_tile_map(&h->tm[i], bufs[i], h->elem, h->G.X, h->G.Y, h->nf);
+    for (int i = 0; i < 8 && ok; ++i)
+      ok = encode_tile_map(&h->tm[i], bufs[i], h->elem, h->G.X, h->G.Y, h->nf, i >= 6);
     h->tma = ok;
   }
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess &&
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+    h->num_sms = sms;
   return SS_OK;
 }
 
 int ss_tma_enabled(const ss_handle* h) { return h && h->tma ? 1 : 0; }
+
+int ss_autotune(ss_handle* h, int iters, float* ms_out) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!h->field || !h->vel) return fail(SS_ERR_STATE, "no Field/Velocity bound");
+  if (h->precision == SS_PLAIN_FP64) return SS_OK;
+  if (iters < 1) iters = 1;
+  rc = dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (h->precision == SS_FP32) return Fused<TH, float>::autotune(h, iters);
+    return Fused<TH, double>::autotune(h, iters);
+  });
+  if (rc) return rc;
+  if (ms_out)
+    for (int m = 0; m < 6; ++m) {
+      ms_out[2 * m] = h->tune_ms[m][0];
+      ms_out[2 * m + 1] = h->tune_ms[m][1];
+    }
+  return take_status(h);
+}
+
+int ss_get_variant(const ss_handle* h, int mode) {
+  if (!h || mode < 0 || mode > 5) return -1;
+  return h->use_pipe[mode];
+}
 
 int ss_step_async(ss_handle* h, int n_steps, double prev_energy, double* energy_traj_dev, double* err_traj_dev) {
   int rc = check_bound(h);

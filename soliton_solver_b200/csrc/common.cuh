@@ -24,13 +24,34 @@ struct Grid {
   double ihx, ihy;      // 1/lsx, 1/lsy
   double ihx2, ihy2;    // 1/lsx^2, 1/lsy^2
   double ih2dA;         // 1/(2 dA)
+  // host-precomputed stencil / time-step constants in both precisions (GK_* slots)
+  double kd[16];
+  float kf[16];
 };
 
-// Theory constants.  Meaning of the slots per theory is documented in theories.cuh.
+// slots of Grid::kd / Grid::kf
+enum {
+  GK_C23HX = 0, GK_MC12HX, GK_C43HX2, GK_MC12HX2, GK_C23HY, GK_MC12HY, GK_C43HY2, GK_MC12HY2, GK_C43HD,
+  GK_MC12HD, GK_DT, GK_MDT, GK_HDT, GK_DT6, GK_SIXTH, GK_COUNT
+};
+
+// Theory constants.  Meaning of the slots per theory is documented in theories.cuh;
+// cf holds the same values rounded to FP32 (filled on the host) so that FP32 kernels
+// use them without conversions.
 struct Phys {
   double c[24];
+  float cf[24];
   int k[12];
 };
+
+template <typename S>
+__device__ __forceinline__ S grid_k(const Grid& G, int i) {
+  if constexpr (sizeof(S) == 4) return G.kf[i]; else return G.kd[i];
+}
+template <typename S>
+__device__ __forceinline__ S phys_k(const Phys& P, int i) {
+  if constexpr (sizeof(S) == 4) return P.cf[i]; else return P.c[i];
+}
 
 // Device-side state of one lattice's flow (lives in the caller's workspace).
 struct StepState {

@@ -22,6 +22,7 @@
 #include <cuda.h>
 
 #include "common.cuh"
+#include "pair.cuh"
 #include "theories.cuh"
 
 namespace ssb {
@@ -39,6 +40,8 @@ struct FlowArgs {
   CUtensorMap tm_phi;  // TMA maps (used when the kernel is instantiated with TMA)
   CUtensorMap tm_vel;
   CUtensorMap tm_l;    // l1 (S3) or l2 (S4)
+  CUtensorMap tm_c1;   // l1 centre tiles (pipelined S4)
+  CUtensorMap tm_c3;   // l3 centre tiles (pipelined S4)
   const R* phi;
   const R* vel;
   const R* la;  // l1 (S3, S4)
@@ -175,7 +178,264 @@ __device__ inline void stage_plain(R* T, const FlowArgs<R>& A, int x0, int y0, i
   }
 }
 
-template <class TH, typename R, int TX, int TY, int NT, bool TMA>
+// Stencil weights pre-scaled by the lattice spacings, as broadcast pairs.
+template <typename V>
+struct PairCoef {
+  using S = typename ScalarOf<V>::type;
+  V c23hx, mc12hx, c43hx2, mc12hx2, c23hy, mc12hy, c43hy2, mc12hy2, c43hd, mc12hd;
+  __device__ explicit PairCoef(const Grid& G)
+      : c23hx(grid_k<S>(G, GK_C23HX)), mc12hx(grid_k<S>(G, GK_MC12HX)), c43hx2(grid_k<S>(G, GK_C43HX2)),
+        mc12hx2(grid_k<S>(G, GK_MC12HX2)), c23hy(grid_k<S>(G, GK_C23HY)), mc12hy(grid_k<S>(G, GK_MC12HY)),
+        c43hy2(grid_k<S>(G, GK_C43HY2)), mc12hy2(grid_k<S>(G, GK_MC12HY2)), c43hd(grid_k<S>(G, GK_C43HD)),
+        mc12hd(grid_k<S>(G, GK_MC12HD)) {}
+};
+
+// Unmasked jet of one component for the site pair (x, y), (x, y+1) whose centre
+// pair starts at `row` in the staged tile (rows HY apart).  Difference form as in
+// d1_stencil / d2_stencil; Dx1 = f(x+1)-f(x-1), Dx2 = f(x+2)-f(x-2) and the y
+// analogues are returned for the FP64 energy.
+template <typename V, typename R, int HY, bool XY>
+__device__ __forceinline__ void pair_jet(const R* row, const PairCoef<V>& k, V& f, V& dx, V& dy, V& dxx, V& dyy,
+                                         V& dxy, V& Dx1, V& Dx2, V& Dy1, V& Dy2) {
+  const V A = ld_pair(row - 2), B = ld_pair(row), C = ld_pair(row + 2);
+  const V xm1 = ld_pair(row - HY), xp1 = ld_pair(row + HY);
+  const V xm2 = ld_pair(row - 2 * HY), xp2 = ld_pair(row + 2 * HY);
+  const V ym1 = shift1(A, B), yp1 = shift1(B, C);
+  f = B;
+  Dx1 = xp1 - xm1;
+  Dx2 = xp2 - xm2;
+  Dy1 = yp1 - ym1;
+  Dy2 = C - A;
+  dx = vfma(Dx1, k.c23hx, Dx2 * k.mc12hx);
+  dy = vfma(Dy1, k.c23hy, Dy2 * k.mc12hy);
+  dxx = vfma((xp1 - B) + (xm1 - B), k.c43hx2, ((xp2 - B) + (xm2 - B)) * k.mc12hx2);
+  dyy = vfma((yp1 - B) + (ym1 - B), k.c43hy2, ((C - B) + (A - B)) * k.mc12hy2);
+  if constexpr (XY) {
+    // main diagonal (x+k, y+k), soliton_solver/core/derivatives.py:105-112
+    const V dp1 = shift1(xp1, ld_pair(row + HY + 2));
+    const V dp2 = ld_pair(row + 2 * HY + 2);
+    const V dm1 = shift1(ld_pair(row - HY - 2), xm1);
+    const V dm2 = ld_pair(row - 2 * HY - 2);
+    const V diag = vfma((dp1 - B) + (dm1 - B), k.c43hd, ((dp2 - B) + (dm2 - B)) * k.mc12hd);
+    dxy = vfma(dxx, V(-0.5), vfma(dyy, V(-0.5), diag));
+  } else {
+    dxy = V(0.0);
+  }
+}
+
+template <typename V>
+__device__ __forceinline__ V mask_lanes(V v, bool m0, bool m1) {
+  using S = typename ScalarOf<V>::type;
+  if (!m0) Lanes<V>::set(v, 0, (S)0);
+  if (!m1) Lanes<V>::set(v, 1, (S)0);
+  return v;
+}
+
+// global pair load / store; `fast` pairs are aligned and both in range
+template <typename V, typename R>
+__device__ __forceinline__ V gload(const R* p, bool fast, bool v1) {
+  using S = typename ScalarOf<V>::type;
+  if (fast) return ld_pair(p);
+  V r(0.0);
+  Lanes<V>::set(r, 0, (S)p[0]);
+  if (v1) Lanes<V>::set(r, 1, (S)p[1]);
+  return r;
+}
+template <typename V, typename R>
+__device__ __forceinline__ void gstore(R* p, V v, bool fast, bool v1) {
+  if (fast) {
+    st_pair(p, v);
+    return;
+  }
+  p[0] = Lanes<V>::get(v, 0);
+  if (v1) p[1] = Lanes<V>::get(v, 1);
+}
+
+// The per-site work of one staged tile.  Each thread owns y-adjacent site pairs;
+// FAST: the tile is interior (every derivative mask true, no halo site) and the
+// lattice row length is even, so pairs are aligned and need no lane masks.
+template <class TH, typename R, int TX, int TY, int NT, bool FAST, int MODE>
+__device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, const R* Praw, const R* Vraw, int x0,
+                                          int y0, bool arrest, double& err_max, const R* C1 = nullptr,
+                                          const R* C3 = nullptr) {
+  using TS = TileShape<TX, TY, NT>;
+  using V = typename PairOf<R>::type;
+  constexpr int NF = TH::NF;
+  constexpr int PAIRS = TY / 2;
+  constexpr int RPP = NT / PAIRS;
+  static_assert(NT % PAIRS == 0 && TX % RPP == 0, "pair mapping");
+  using S = typename ScalarOf<V>::type;
+  const Grid& G = A.G;
+  const long long N = G.N;
+  const PairCoef<V> kc(G);
+  const V mdt(grid_k<S>(G, GK_MDT));
+  S emax = -INFINITY;
+  const int j = threadIdx.x % PAIRS;
+  const int lxg = threadIdx.x / PAIRS;
+#pragma unroll 1
+  for (int pass = 0; pass < TX / RPP; ++pass) {
+    const int lx = lxg + pass * RPP;
+    const int gx = x0 + lx, gy = y0 + 2 * j;
+    bool v1 = true;
+    Masks m0{true, true, true}, m1{true, true, true};
+    if (!FAST) {
+      if (gx >= G.X || gy >= G.Y) continue;
+      v1 = gy + 1 < G.Y;
+      m0 = site_masks(G, gx, gy);
+      m1 = site_masks(G, gx, gy + 1);
+      if (!v1) m1 = Masks{false, false, false};
+    }
+    const int toff = (lx + 2) * TS::HY + TS::YOFF + 2 * j;
+    const long long sidx = (long long)gx * G.Y + gy;
+
+    Jet<V, NF> J;
+    V Dx1[NF], Dx2[NF], Dy1[NF], Dy2[NF];
+#pragma unroll
+    for (int a = 0; a < NF; ++a) {
+      pair_jet<V, R, TS::HY, TH::NEED_XY>(T + a * TS::PLANE + toff, kc, J.f[a], J.dx[a], J.dy[a], J.dxx[a],
+                                                  J.dyy[a], J.dxy[a], Dx1[a], Dx2[a], Dy1[a], Dy2[a]);
+      if (!FAST) {
+        J.dx[a] = mask_lanes(J.dx[a], m0.x, m1.x);
+        J.dy[a] = mask_lanes(J.dy[a], m0.y, m1.y);
+        J.dxx[a] = mask_lanes(J.dxx[a], m0.x, m1.x);
+        J.dyy[a] = mask_lanes(J.dyy[a], m0.y, m1.y);
+        J.dxy[a] = mask_lanes(J.dxy[a], m0.xy, m1.xy);
+      }
+    }
+
+    V g[NF];
+    TH::gradient(J, A.P, g);
+    if (TH::HALO_ZERO && !FAST) {
+      const bool e0 = gx < G.halo || gx > G.X - G.halo - 1 || gy < G.halo || gy > G.Y - G.halo - 1;
+      const bool e1 = gx < G.halo || gx > G.X - G.halo - 1 || gy + 1 < G.halo || gy + 1 > G.Y - G.halo - 1;
+#pragma unroll
+      for (int a = 0; a < NF; ++a) g[a] = mask_lanes(g[a], !e0, !e1);
+    }
+    if (TH::CONSTRAINED) {  // project_orthogonal_magnetization (chiral_magnet/kernels.py:86-122)
+      V lm = g[0] * J.f[0];
+#pragma unroll
+      for (int a = 1; a < TH::NMAG; ++a) lm = vfma(g[a], J.f[a], lm);
+      const V mlm = -lm;
+#pragma unroll
+      for (int a = 0; a < TH::NMAG; ++a) g[a] = vfma(mlm, J.f[a], g[a]);
+    }
+    if constexpr (MODE == M_GRAD) {
+#pragma unroll
+      for (int a = 0; a < NF; ++a) {
+        if (A.out_eg) gstore<V, R>(A.out_eg + a * N + sidx, g[a], FAST, v1);
+        if (A.out_l) gstore<V, R>(A.out_l + a * N + sidx, mdt * g[a], FAST, v1);
+      }
+    } else if constexpr (MODE != M_S4) {
+#pragma unroll
+      for (int a = 0; a < NF; ++a) gstore<V, R>(A.out_l + a * N + sidx, mdt * g[a], FAST, v1);
+    } else {
+      // RK4 finalize (core/integrator.py:151-189) fused with stage 4:
+      // V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,  phi' = phi + dt V + dt (l1 + l2 + l3)/6
+      V Pn[NF], Vn[NF];
+      const V sixth(grid_k<S>(G, GK_SIXTH)), two(2.0), dtv(grid_k<S>(G, GK_DT)), dt6(grid_k<S>(G, GK_DT6));
+#pragma unroll
+      for (int a = 0; a < NF; ++a) {
+        const long long idx = a * N + sidx;
+        const V p = Praw ? ld_pair(Praw + a * TS::PLANE + toff) : gload<V, R>(A.phi + idx, FAST, v1);
+        const V v = arrest ? V(0.0) : (Vraw ? ld_pair(Vraw + a * TS::PLANE + toff) : gload<V, R>(A.vel + idx, FAST, v1));
+        const int coff = a * TX * TY + lx * TY + 2 * j;
+        const V l1 = C1 ? ld_pair(C1 + coff) : gload<V, R>(A.la + idx, FAST, v1);
+        const V l2 = gload<V, R>(A.lb + idx, FAST, v1);
+        const V l3 = C3 ? ld_pair(C3 + coff) : gload<V, R>(A.lc + idx, FAST, v1);
+        const V l4 = mdt * g[a];
+        Vn[a] = vfma(sixth, vfma(two, l3, vfma(two, l2, l1)) + l4, v);
+        Pn[a] = vfma(dt6, (l1 + l2) + l3, vfma(dtv, v, p));
+        emax = fmax(emax, Lanes<V>::get(g[a], 0));
+        if (v1) emax = fmax(emax, Lanes<V>::get(g[a], 1));
+      }
+      if (TH::CONSTRAINED && G.unit_mag) {
+        // compute_norm_magnetization + project_orthogonal_magnetization (kernels.py:48-122)
+        V s2 = Pn[0] * Pn[0];
+#pragma unroll
+        for (int a = 1; a < TH::NMAG; ++a) s2 = vfma(Pn[a], Pn[a], s2);
+        V inv(1.0);
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+          const S s = sqrt(Lanes<V>::get(s2, l));
+          if (s != (S)0) Lanes<V>::set(inv, l, (S)1 / s);
+        }
+#pragma unroll
+        for (int a = 0; a < TH::NMAG; ++a) Pn[a] = Pn[a] * inv;
+        V lm = Vn[0] * Pn[0];
+#pragma unroll
+        for (int a = 1; a < TH::NMAG; ++a) lm = vfma(Vn[a], Pn[a], lm);
+        const V mlm = -lm;
+#pragma unroll
+        for (int a = 0; a < TH::NMAG; ++a) Vn[a] = vfma(mlm, Pn[a], Vn[a]);
+      }
+#pragma unroll
+      for (int a = 0; a < NF; ++a) {
+        gstore<V, R>(A.phi_out + a * N + sidx, Pn[a], FAST, v1);
+        gstore<V, R>(A.vel_out + a * N + sidx, Vn[a], FAST, v1);
+      }
+    }
+  }
+  if (MODE == M_S4) err_max = fmax(err_max, (double)emax);
+}
+
+// FP64 energy of the staged field (T_1 = phi): first derivatives from the exact
+// differences f(x+k) - f(x-k) of the stored values, evaluated in FP64.
+template <class TH, typename R, int TX, int TY, int NT, bool FAST, typename E = R>
+__device__ __forceinline__ double energy_tile(const FlowArgs<R>& A, const E* T, int x0, int y0) {
+  using TS = TileShape<TX, TY, NT>;
+  using V = typename PairOf<E>::type;
+  constexpr int NF = TH::NF;
+  constexpr int PAIRS = TY / 2;
+  constexpr int RPP = NT / PAIRS;
+  const Grid& G = A.G;
+  const double c23x = FD::c23 * G.ihx, c12x = FD::c12 * G.ihx;
+  const double c23y = FD::c23 * G.ihy, c12y = FD::c12 * G.ihy;
+  const int j = threadIdx.x % PAIRS;
+  const int lxg = threadIdx.x / PAIRS;
+  double e_acc = 0.0;
+#pragma unroll 1
+  for (int pass = 0; pass < TX / RPP; ++pass) {
+    const int lx = lxg + pass * RPP;
+    const int gx = x0 + lx, gy = y0 + 2 * j;
+    bool v1 = true;
+    Masks m0{true, true, true}, m1{true, true, true};
+    if (!FAST) {
+      if (gx >= G.X || gy >= G.Y) continue;
+      v1 = gy + 1 < G.Y;
+      m0 = site_masks(G, gx, gy);
+      m1 = site_masks(G, gx, gy + 1);
+    }
+    const int toff = (lx + 2) * TS::HY + TS::YOFF + 2 * j;
+    Jet1<double, NF> J0, J1;
+#pragma unroll
+    for (int a = 0; a < NF; ++a) {
+      const E* row = T + a * TS::PLANE + toff;
+      // six y values cover both sites' y stencils; converted once
+      const V Ap = ld_pair(row - 2), B = ld_pair(row), C = ld_pair(row + 2);
+      const double y_2 = (double)Lanes<V>::get(Ap, 0), y_1 = (double)Lanes<V>::get(Ap, 1);
+      const double y0v = (double)Lanes<V>::get(B, 0), y1v = (double)Lanes<V>::get(B, 1);
+      const double y2 = (double)Lanes<V>::get(C, 0), y3 = (double)Lanes<V>::get(C, 1);
+      const V xp1 = ld_pair(row + TS::HY), xm1 = ld_pair(row - TS::HY);
+      const V xp2 = ld_pair(row + 2 * TS::HY), xm2 = ld_pair(row - 2 * TS::HY);
+#pragma unroll
+      for (int l = 0; l < 2; ++l) {
+        Jet1<double, NF>& J = l ? J1 : J0;
+        const Masks& m = l ? m1 : m0;
+        const double ddx = (c23x * ((double)Lanes<V>::get(xp1, l) - (double)Lanes<V>::get(xm1, l)) -
+                            c12x * ((double)Lanes<V>::get(xp2, l) - (double)Lanes<V>::get(xm2, l)));
+        const double ddy = l ? (c23y * (y2 - y0v) - c12y * (y3 - y_1)) : (c23y * (y1v - y_1) - c12y * (y2 - y_2));
+        J.f[a] = l ? y1v : y0v;
+        J.dx[a] = m.x ? ddx : 0.0;
+        J.dy[a] = m.y ? ddy : 0.0;
+      }
+    }
+    e_acc += TH::energy(J0, A.P, G.dA);
+    if (v1) e_acc += TH::energy(J1, A.P, G.dA);
+  }
+  return e_acc;
+}
+
+template <class TH, typename R, int TX, int TY, int NT, bool TMA, int MODE>
 __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowArgs<R> A) {
   using TS = TileShape<TX, TY, NT>;
   constexpr int NF = TH::NF;
@@ -190,15 +450,13 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
   __shared__ __align__(8) uint64_t bar;
 
   const Grid& G = A.G;
-  const int mode = A.mode;
+  constexpr int mode = MODE;
   const int tiles_y = (G.Y + TY - 1) / TY;
   const int x0 = (blockIdx.x / tiles_y) * TX;
   const int y0 = (blockIdx.x % tiles_y) * TY;
-  const long long N = G.N;
   StepState* st = A.st;
   const bool arrest = (mode == M_S2 || mode == M_S3 || mode == M_S4) && (st->arrest != 0);
-  const bool do_energy = A.with_energy != 0;
-  const R dt = (R)G.dt;
+  const bool do_energy = (MODE == M_S1 || MODE == M_ENERGY) && A.with_energy != 0;
 
   if (A.init_state && blockIdx.x == 0 && threadIdx.x == 0) {
     st->arrest = 0;
@@ -229,10 +487,25 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
       // combine in place into the last staged buffer (OOB entries are zero in all)
       R* dst = need_l ? B2 : (need_v ? B1 : B0);
       if (dst != B0) {
-        for (int i = threadIdx.x; i < BUF; i += NT) {
-          const R v = need_v ? B1[i] : (R)0;
-          const R w = need_l ? B2[i] : (R)0;
-          dst[i] = stage_value<R>(mode, B0[i], v, w, dt);
+        using V = typename PairOf<R>::type;
+        const V half(0.5), hdt(grid_k<R>(G, GK_HDT)), dtv(grid_k<R>(G, GK_DT));
+        for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
+          V p0, p1, v0(0.0), v1(0.0), w0(0.0), w1(0.0);
+          ld_quad(B0 + i, p0, p1);
+          if (need_v) ld_quad(B1 + i, v0, v1);
+          if (need_l) ld_quad(B2 + i, w0, w1);
+          V t0, t1;
+          if (mode == M_S2) {
+            t0 = vfma(hdt, v0, p0);
+            t1 = vfma(hdt, v1, p1);
+          } else if (mode == M_S3) {
+            t0 = vfma(hdt, vfma(half, w0, v0), p0);
+            t1 = vfma(hdt, vfma(half, w1, v1), p1);
+          } else {
+            t0 = vfma(dtv, vfma(half, w0, v0), p0);
+            t1 = vfma(dtv, vfma(half, w1, v1), p1);
+          }
+          st_quad(dst + i, t0, t1);
         }
         __syncthreads();
       }
@@ -243,102 +516,45 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
     __syncthreads();
   }
 
-  const Inv<R> iv(G);
-  const Inv<double> ivd(G);
-  const int ly = threadIdx.x % TY;
-  const int lxg = threadIdx.x / TY;
   double e_acc = 0.0;
   double err_max = -INFINITY;
-
-#pragma unroll 1
-  for (int s = 0; s < TS::SITES_PER_THREAD; ++s) {
-    const int lx = lxg + s * TS::ROWS_PER_PASS;
-    const int gx = x0 + lx, gy = y0 + ly;
-    if (gx >= G.X || gy >= G.Y) continue;
-    const Masks mk = site_masks(G, gx, gy);
-    const R* base = T + (lx + 2) * TS::HY + (ly + TS::YOFF);
-
+  const R* Praw = nullptr;
+  const R* Vraw = nullptr;
+  if constexpr (TMA) {
+    if (mode == M_S4) {
+      Praw = B0;
+      Vraw = arrest ? nullptr : B1;
+    }
+  }
+  const bool fast = (G.Y % 2 == 0) && x0 >= G.halo + 1 && x0 + TX - 1 <= G.X - G.halo - 2 && y0 >= G.halo + 1 &&
+                    y0 + TY - 1 <= G.Y - G.halo - 2;
+  if constexpr (MODE != M_ENERGY) {
+    if (fast)
+      grad_tile<TH, R, TX, TY, NT, true, MODE>(A, T, Praw, Vraw, x0, y0, arrest, err_max);
+    else
+      grad_tile<TH, R, TX, TY, NT, false, MODE>(A, T, Praw, Vraw, x0, y0, arrest, err_max);
+  }
+  if constexpr (MODE == M_S1 || MODE == M_ENERGY) {
     if (do_energy) {
-      Jet1<double, NF> J1;
-#pragma unroll
-      for (int a = 0; a < NF; ++a) {
-        const R* pa = base + a * TS::PLANE;
-        auto acc = [pa](int dx, int dy) -> double { return (double)pa[dx * TS::HY + dy]; };
-        fill_jet1_comp<double>(acc, mk, ivd, J1.f[a], J1.dx[a], J1.dy[a]);
-      }
-      e_acc += TH::energy(J1, A.P, G.dA);
-    }
-    if (mode == M_ENERGY) continue;
-
-    Jet<R, NF> J;
-#pragma unroll
-    for (int a = 0; a < NF; ++a) {
-      const R* pa = base + a * TS::PLANE;
-      auto acc = [pa](int dx, int dy) -> R { return pa[dx * TS::HY + dy]; };
-      fill_jet_comp<R>(acc, mk, iv, J.f[a], J.dx[a], J.dy[a], J.dxx[a], J.dyy[a], J.dxy[a], TH::NEED_XY);
-    }
-    R g[NF];
-    TH::gradient(J, A.P, g);
-    if (TH::HALO_ZERO) {
-      const bool edge = gx < G.halo || gx > G.X - G.halo - 1 || gy < G.halo || gy > G.Y - G.halo - 1;
-      if (edge) {
-#pragma unroll
-        for (int a = 0; a < NF; ++a) g[a] = (R)0;
-      }
-    }
-    if (TH::CONSTRAINED) {  // project_orthogonal_magnetization (chiral_magnet/kernels.py:86-122)
-      R lm = (R)0;
-#pragma unroll
-      for (int a = 0; a < TH::NMAG; ++a) lm += g[a] * J.f[a];
-#pragma unroll
-      for (int a = 0; a < TH::NMAG; ++a) g[a] -= lm * J.f[a];
-    }
-    const long long sidx = (long long)gx * G.Y + gy;
-    if (mode == M_GRAD) {
-#pragma unroll
-      for (int a = 0; a < NF; ++a) {
-        if (A.out_eg) A.out_eg[a * N + sidx] = g[a];
-        if (A.out_l) A.out_l[a * N + sidx] = -dt * g[a];
-      }
-    } else if (mode != M_S4) {
-#pragma unroll
-      for (int a = 0; a < NF; ++a) A.out_l[a * N + sidx] = -dt * g[a];
-    } else {
-      // RK4 finalize (core/integrator.py:151-189) fused with stage 4
-      R Pn[NF], Vn[NF];
-      const R sixth = (R)(1.0 / 6.0), half = (R)0.5, two = (R)2;
-#pragma unroll
-      for (int a = 0; a < NF; ++a) {
-        const long long idx = a * N + sidx;
-        const R v = arrest ? (R)0 : A.vel[idx];
-        const R p = A.phi[idx];
-        const R l1 = A.la[idx], l2 = A.lb[idx], l3 = A.lc[idx];
-        const R l4 = -dt * g[a];
-        const R k1 = dt * v, k2 = dt * (v + half * l1), k3 = dt * (v + half * l2), k4 = dt * (v + l3);
-        Vn[a] = v + sixth * (l1 + two * l2 + two * l3 + l4);
-        Pn[a] = p + sixth * (k1 + two * k2 + two * k3 + k4);
-        err_max = fmax(err_max, (double)g[a]);
-      }
-      if (TH::CONSTRAINED && G.unit_mag) {
-        // compute_norm_magnetization + project_orthogonal_magnetization (kernels.py:48-122)
-        R s2 = (R)0;
-#pragma unroll
-        for (int a = 0; a < TH::NMAG; ++a) s2 += Pn[a] * Pn[a];
-        const R s = sqrt(s2);
-        if (s != (R)0) {
-#pragma unroll
-          for (int a = 0; a < TH::NMAG; ++a) Pn[a] /= s;
+      if constexpr (sizeof(R) == 4) {
+        // convert the staged FP32 tile to FP64 once (each value then serves all the
+        // stencils it enters without further conversions); placed after B0
+        double* Td = reinterpret_cast<double*>(B1);
+        for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
+          const float4 v = *reinterpret_cast<const float4*>(T + i);
+          *reinterpret_cast<double2*>(Td + i) = make_double2((double)v.x, (double)v.y);
+          *reinterpret_cast<double2*>(Td + i + 2) = make_double2((double)v.z, (double)v.w);
         }
-        R lm = (R)0;
-#pragma unroll
-        for (int a = 0; a < TH::NMAG; ++a) lm += Vn[a] * Pn[a];
-#pragma unroll
-        for (int a = 0; a < TH::NMAG; ++a) Vn[a] -= lm * Pn[a];
-      }
-#pragma unroll
-      for (int a = 0; a < NF; ++a) {
-        A.phi_out[a * N + sidx] = Pn[a];
-        A.vel_out[a * N + sidx] = Vn[a];
+        __syncthreads();
+        if (fast)
+          e_acc = energy_tile<TH, R, TX, TY, NT, true, double>(A, Td, x0, y0);
+        else
+          e_acc = energy_tile<TH, R, TX, TY, NT, false, double>(A, Td, x0, y0);
+      } else {
+        if (fast)
+          e_acc = energy_tile<TH, R, TX, TY, NT, true>(A, T, x0, y0);
+        else
+          e_acc = energy_tile<TH, R, TX, TY, NT, false>(A, T, x0, y0);
       }
     }
   }
@@ -376,6 +592,206 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
   }
   if (threadIdx.x == 0) {
     if (mode == M_S4) {
+      const double err = dec_max(atomicExch(&st->err_enc, 0ULL));
+      if (A.err_traj && A.err_idx >= 0) A.err_traj[A.err_idx] = err;
+    }
+    st->ticket = 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent, TMA-pipelined form of flow_kernel (FP32 fields): one CTA per SM
+// walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ... through a ring of STAGES
+// shared-memory slots, so the bulk tensor loads of the next tiles are in flight
+// while the current tile is computed.  Stage 4 also stages the centre tiles of l1
+// and l3.  Energy partials are per CTA in tile order (deterministic for a fixed grid).
+// ---------------------------------------------------------------------------
+template <int MODE>
+__host__ __device__ constexpr int pipe_halo_buffers() {
+  return MODE == M_S2 ? 2 : (MODE == M_S3 || MODE == M_S4) ? 3 : 1;
+}
+template <int MODE>
+__host__ __device__ constexpr int pipe_centre_buffers() {
+  return MODE == M_S4 ? 2 : 0;
+}
+template <typename R, int NF, int TX, int TY, int MODE>
+__host__ __device__ constexpr size_t pipe_slot_bytes() {
+  return tile_buf_bytes<R, NF, TX, TY>() * pipe_halo_buffers<MODE>() +
+         sizeof(R) * NF * TX * TY * pipe_centre_buffers<MODE>();
+}
+
+template <class TH, typename R, int TX, int TY, int NT, int MODE, int STAGES>
+__global__ void __launch_bounds__(NT, 1) flow_kernel_pipe(const __grid_constant__ FlowArgs<R> A) {
+  using TS = TileShape<TX, TY, NT>;
+  constexpr int NF = TH::NF;
+  constexpr int BUF = NF * TS::PLANE;             // elements of one halo buffer
+  constexpr int CBUF = NF * TX * TY;              // elements of one centre buffer
+  constexpr int SLOT = BUF * pipe_halo_buffers<MODE>() + CBUF * pipe_centre_buffers<MODE>();
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  R* ring = reinterpret_cast<R*>(smem_raw);
+  __shared__ double red[NT / 32];
+  __shared__ double sh_s[NT], sh_c[NT];
+  __shared__ int am_last;
+  __shared__ int timed_out;
+  __shared__ __align__(8) uint64_t full[STAGES];
+
+  const Grid& G = A.G;
+  const int tiles_y = (G.Y + TY - 1) / TY;
+  const int ntiles = ((G.X + TX - 1) / TX) * tiles_y;
+  StepState* st = A.st;
+  const bool arrest = (MODE == M_S2 || MODE == M_S3 || MODE == M_S4) && (st->arrest != 0);
+  const bool do_energy = (MODE == M_S1 || MODE == M_ENERGY) && A.with_energy != 0;
+  const bool need_v = (MODE == M_S2 || MODE == M_S3 || MODE == M_S4) && !arrest;
+  constexpr bool need_l = MODE == M_S3 || MODE == M_S4;
+  const uint32_t bytes = (uint32_t)(sizeof(R) * (BUF * (1 + (need_v ? 1 : 0) + (need_l ? 1 : 0)) +
+                                                 CBUF * pipe_centre_buffers<MODE>()));
+
+  if (A.init_state && blockIdx.x == 0 && threadIdx.x == 0) {
+    st->arrest = 0;
+    if (!isnan(A.prev_energy)) st->E_last = A.prev_energy;
+  }
+  auto issue = [&](int slot, int tile) {
+    R* base = ring + slot * SLOT;
+    const int x0 = (tile / tiles_y) * TX, y0 = (tile % tiles_y) * TY;
+    mbar_expect_tx(&full[slot], bytes);
+    tma_load_3d(base, &A.tm_phi, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
+    if (need_v) tma_load_3d(base + BUF, &A.tm_vel, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
+    if (need_l) tma_load_3d(base + 2 * BUF, &A.tm_l, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
+    if (MODE == M_S4) {
+      tma_load_3d(base + 3 * BUF, &A.tm_c1, y0, x0, 0, &full[slot]);
+      tma_load_3d(base + 3 * BUF + CBUF, &A.tm_c3, y0, x0, 0, &full[slot]);
+    }
+  };
+  if (threadIdx.x == 0) {
+    timed_out = 0;
+    for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      const int t = blockIdx.x + s * gridDim.x;
+      if (t < ntiles) issue(s, t);
+    }
+  }
+
+  double e_acc = 0.0;
+  double err_max = -INFINITY;
+  int k = 0;
+  // tile coordinates advanced without a division per tile
+  const int dq = gridDim.x / tiles_y, dr = gridDim.x % tiles_y;
+  int tx = blockIdx.x / tiles_y, ty = blockIdx.x % tiles_y;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+    const int slot = k % STAGES;
+    const uint32_t parity = (uint32_t)((k / STAGES) & 1);
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&full[slot], parity));
+    if (!ok) {
+      // record, then wait (bounded) for every load still in flight before leaving
+      if (threadIdx.x == 0) atomicExch(&st->status, (int)ST_TIMEOUT);
+      for (int s = 0; s < STAGES; ++s) {
+        const int kk = k + s;
+        if (blockIdx.x + kk * gridDim.x < ntiles) mbar_wait_bounded(&full[kk % STAGES], (uint32_t)((kk / STAGES) & 1));
+      }
+      return;
+    }
+    R* base = ring + slot * SLOT;
+    R* B0 = base;
+    R* B1 = base + BUF;
+    R* B2 = base + 2 * BUF;
+    const int x0 = tx * TX, y0 = ty * TY;
+    tx += dq;
+    ty += dr;
+    if (ty >= tiles_y) {
+      ty -= tiles_y;
+      ++tx;
+    }
+    R* T = B0;
+    if (MODE == M_S2 || MODE == M_S3 || MODE == M_S4) {
+      R* dst = need_l ? B2 : (need_v ? B1 : B0);
+      if (dst != B0) {
+        using V = typename PairOf<R>::type;
+        const V half(0.5), hdt(grid_k<R>(G, GK_HDT)), dtv(grid_k<R>(G, GK_DT));
+        for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
+          V p0, p1, v0(0.0), v1(0.0), w0(0.0), w1(0.0);
+          ld_quad(B0 + i, p0, p1);
+          if (need_v) ld_quad(B1 + i, v0, v1);
+          if (need_l) ld_quad(B2 + i, w0, w1);
+          V t0, t1;
+          if (MODE == M_S2) {
+            t0 = vfma(hdt, v0, p0);
+            t1 = vfma(hdt, v1, p1);
+          } else if (MODE == M_S3) {
+            t0 = vfma(hdt, vfma(half, w0, v0), p0);
+            t1 = vfma(hdt, vfma(half, w1, v1), p1);
+          } else {
+            t0 = vfma(dtv, vfma(half, w0, v0), p0);
+            t1 = vfma(dtv, vfma(half, w1, v1), p1);
+          }
+          st_quad(dst + i, t0, t1);
+        }
+        __syncthreads();
+      }
+      T = dst;
+    }
+    const R* Praw = MODE == M_S4 ? B0 : nullptr;
+    const R* Vraw = (MODE == M_S4 && !arrest) ? B1 : nullptr;
+    const R* C1 = MODE == M_S4 ? base + 3 * BUF : nullptr;
+    const R* C3 = MODE == M_S4 ? base + 3 * BUF + CBUF : nullptr;
+    const bool fast = (G.Y % 2 == 0) && x0 >= G.halo + 1 && x0 + TX - 1 <= G.X - G.halo - 2 &&
+                      y0 >= G.halo + 1 && y0 + TY - 1 <= G.Y - G.halo - 2;
+    if constexpr (MODE != M_ENERGY) {
+      if (fast)
+        grad_tile<TH, R, TX, TY, NT, true, MODE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3);
+      else
+        grad_tile<TH, R, TX, TY, NT, false, MODE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3);
+    }
+    if constexpr (MODE == M_S1 || MODE == M_ENERGY) {
+      if (do_energy) {
+        if (fast)
+          e_acc += energy_tile<TH, R, TX, TY, NT, true>(A, T, x0, y0);
+        else
+          e_acc += energy_tile<TH, R, TX, TY, NT, false>(A, T, x0, y0);
+      }
+    }
+    __syncthreads();  // every thread is done with this slot
+    if (threadIdx.x == 0) {
+      const int nt = t + STAGES * gridDim.x;
+      if (nt < ntiles) issue(slot, nt);
+    }
+  }
+
+  // ---- reductions (as flow_kernel) ----------------------------------------
+  const bool need_ticket = do_energy || MODE == M_S4;
+  if (!need_ticket) return;
+  if (do_energy) {
+    const double bs = block_sum_fixed<NT>(e_acc, red);
+    if (threadIdx.x == 0) A.partial[blockIdx.x] = bs;
+  }
+  if (MODE == M_S4) {
+    const double bm = block_max<NT>(err_max, red);
+    if (threadIdx.x == 0 && bm > -INFINITY) atomicMax(&st->err_enc, enc_max(bm));
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned tk = atomicAdd(&st->ticket, 1u);
+    am_last = (tk == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  if (do_energy) {
+    const double E = fixed_order_sum<NT>(A.partial, gridDim.x, sh_s, sh_c);
+    if (threadIdx.x == 0) {
+      st->scalar = E;
+      if (!isfinite(E)) st->status = 3;
+      if (A.E_traj && A.E_idx >= 0) A.E_traj[A.E_idx] = E;
+      if (A.arrest_update) {
+        st->arrest = (G.killkinen && E > st->E_last) ? 1 : 0;
+        st->E_last = E;
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    if (MODE == M_S4) {
       const double err = dec_max(atomicExch(&st->err_enc, 0ULL));
       if (A.err_traj && A.err_idx >= 0) A.err_traj[A.err_idx] = err;
     }

@@ -13,10 +13,17 @@
 #pragma once
 
 #include "common.cuh"
+#include "pair.cuh"
 
 namespace ssb {
 
 enum { CH_SKYRMION = 0, CH_MAGNETIC = 1, CH_VORTEX = 2 };
+
+// constant slot i of P as R (scalar or broadcast pair) in R's precision
+template <typename R>
+__device__ __forceinline__ R pk(const Phys& P, int i) {
+  return R(phys_k<typename ScalarOf<R>::type>(P, i));
+}
 enum { CP_KAPPA = 0, CP_MPI = 1, CP_LAMBDA = 2, CP_COUP_K = 3, CP_COUP_H = 4, CP_COUP_MU = 5 };
 
 // m.(dx m x dy m) dA / 4pi  (chiral_magnet/kernels.py:254-291, baby_skyrme/kernels.py:237-270)
@@ -38,32 +45,41 @@ struct ChiralMagnet {
   static constexpr bool CONSTRAINED = true, HALO_ZERO = true, NEED_XY = false;
 
   // do_gradient_step_point, kernels.py:398-503 (halo zeroing and projection are
-  // applied by the caller, kernels.py:505-511)
+  // applied by the caller, kernels.py:505-511).  Constants are pre-scaled so every
+  // term is one fused multiply-add; R is a scalar or a packed pair of sites.
+  // derived slots filled on the host (ChiralMagnet::derive):
+  //   c[12] -2 D10  c[13] -2 D11  c[14] 2 D00  c[15] 2 D01  c[16] 2 D10  c[17] 2 D11
+  //   c[18] -2 D00  c[19] -2 D01  c[20] -2 coup_K
+  static void derive(Phys& P) {
+    P.c[12] = -2.0 * P.c[5]; P.c[13] = -2.0 * P.c[6]; P.c[14] = 2.0 * P.c[3]; P.c[15] = 2.0 * P.c[4];
+    P.c[16] = 2.0 * P.c[5]; P.c[17] = 2.0 * P.c[6]; P.c[18] = -2.0 * P.c[3]; P.c[19] = -2.0 * P.c[4];
+    P.c[20] = -2.0 * P.c[0];
+  }
   template <typename R>
   __device__ static inline void gradient(const Jet<R, NF>& J, const Phys& P, R g[NF]) {
-    const R cK = (R)P.c[0], ch = (R)P.c[1], cmu = (R)P.c[2];
-    const R D00 = (R)P.c[3], D01 = (R)P.c[4], D10 = (R)P.c[5], D11 = (R)P.c[6];
+    const double D00 = P.c[3], D01 = P.c[4], D10 = P.c[5], D11 = P.c[6];
 #pragma unroll
     for (int a = 0; a < 3; ++a) g[a] = -(J.dxx[a] + J.dyy[a]);
-    g[3] = (R)0;
-    if (P.c[3] != 0.0 || P.c[4] != 0.0 || P.c[5] != 0.0 || P.c[6] != 0.0) {
+    g[3] = R(0.0);
+    if (D00 != 0.0 || D01 != 0.0 || D10 != 0.0 || D11 != 0.0) {
       // 2 sum_{ij} D_ij eps(j,k,l) d_i m_l  in the reference's (i, j) loop order
-      if (P.c[5] != 0.0) g[0] -= (R)2 * D10 * J.dx[2];
-      if (P.c[6] != 0.0) g[0] -= (R)2 * D11 * J.dy[2];
-      g[1] += (R)2 * D00 * J.dx[2];
-      if (P.c[4] != 0.0) g[1] += (R)2 * D01 * J.dy[2];
-      if (P.c[5] != 0.0) g[2] += (R)2 * D10 * J.dx[0];
-      if (P.c[6] != 0.0) g[2] += (R)2 * D11 * J.dy[0];
-      g[2] -= (R)2 * D00 * J.dx[1];
-      if (P.c[4] != 0.0) g[2] -= (R)2 * D01 * J.dy[1];
+      if (D10 != 0.0) g[0] = vfma(pk<R>(P, 12), J.dx[2], g[0]);
+      if (D11 != 0.0) g[0] = vfma(pk<R>(P, 13), J.dy[2], g[0]);
+      g[1] = vfma(pk<R>(P, 14), J.dx[2], g[1]);
+      if (D01 != 0.0) g[1] = vfma(pk<R>(P, 15), J.dy[2], g[1]);
+      if (D10 != 0.0) g[2] = vfma(pk<R>(P, 16), J.dx[0], g[2]);
+      if (D11 != 0.0) g[2] = vfma(pk<R>(P, 17), J.dy[0], g[2]);
+      g[2] = vfma(pk<R>(P, 18), J.dx[1], g[2]);
+      if (D01 != 0.0) g[2] = vfma(pk<R>(P, 19), J.dy[1], g[2]);
     }
-    g[2] -= ch;
-    g[2] -= (R)2 * cK * J.f[2];
+    // Zeeman and anisotropy: g_z -= coup_h + 2 coup_K m_z
+    g[2] = vfma(pk<R>(P, 20), J.f[2], g[2] - pk<R>(P, 1));
     if (P.k[0]) {
+      const R cmu = pk<R>(P, 2);
       g[0] += J.dx[3];
-      g[3] += cmu * J.dx[0] - J.dxx[3];
+      g[3] = vfma(cmu, J.dx[0], g[3]) - J.dxx[3];
       g[1] += J.dy[3];
-      g[3] += cmu * J.dy[1] - J.dyy[3];
+      g[3] = vfma(cmu, J.dy[1], g[3]) - J.dyy[3];
     }
   }
 
@@ -125,16 +141,39 @@ struct BabySkyrme {
   static constexpr int NF = 3, NMAG = 3;
   static constexpr bool CONSTRAINED = true, HALO_ZERO = false, NEED_XY = true;
 
-  template <typename R>
-  __device__ static inline R rpow(R a, R b) {
-    if constexpr (sizeof(R) == 8) return pow(a, b); else return powf(a, b);
+  template <typename S>
+  __device__ static inline S spow(S a, S b) {
+    if constexpr (sizeof(S) == 8) return pow(a, b); else return powf(a, b);
+  }
+
+  // Broken-potential gradient terms at one site (baby_skyrme/kernels.py:427-446)
+  template <typename S>
+  __device__ static inline void broken(S m1, S m2, S m3, S mpi2, int N, S& g0, S& g1, S& g2) {
+    const S r2 = m1 * m1 + m2 * m2;
+    const S theta = atan2(m2, m1);
+    const S rN2 = spow<S>(r2, (S)(0.5 * N));
+    const S rN = spow<S>(r2, (S)(1.0 * N));
+    const S c = cos((S)N * theta), s = sin((S)N * theta);
+    const S norm1mzN = (S)1 - (S)2 * c * rN2 + rN;
+    const S denom = sqrt(norm1mzN);
+    if (denom != (S)0 && r2 != (S)0) {
+      const S pref = (S)2 * mpi2 * (S)N * sqrt(norm1mzN) * spow<S>(r2, (S)(-1.0 + 0.5 * N)) * ((S)-1 + m3) / denom;
+      g0 += pref * (s * m2 + m1 * (c - rN2));
+      g1 += -pref * (s * m1 + m2 * (-c + rN2));
+    }
+    g2 -= mpi2 * norm1mzN;
+  }
+
+  // derived slots: c[2] mpi^2, c[3] kappa^2
+  static void derive(Phys& P) {
+    P.c[2] = P.c[0] * P.c[0];
+    P.c[3] = P.c[1] * P.c[1];
   }
 
   // do_gradient_step_point, kernels.py:308-458 (projection applied by the caller)
   template <typename R>
   __device__ static inline void gradient(const Jet<R, NF>& J, const Phys& P, R g[NF]) {
-    const R mpi = (R)P.c[0], mpi2 = mpi * mpi;
-    const R kappa = (R)P.c[1], kappa2 = kappa * kappa;
+    const R mpi2 = pk<R>(P, 2), kappa2 = pk<R>(P, 3);
     const R m1 = J.f[0], m2 = J.f[1], m3 = J.f[2];
     const R F00 = J.dx[0], F01 = J.dx[1], F02 = J.dx[2];
     const R F10 = J.dy[0], F11 = J.dy[1], F12 = J.dy[2];
@@ -184,20 +223,17 @@ struct BabySkyrme {
       g2 -= (R)16 * mpi2 * (-(m1 * m1 * m1) + (R)3 * m1 * (m2 * m2) + ((R)1 - (R)3 * m3) * ((R)1 - (R)3 * m3));
     }
     if (P.k[6]) {
-      const int N = P.k[8];
-      const R r2 = m1 * m1 + m2 * m2;
-      const R theta = atan2(m2, m1);
-      const R rN2 = rpow<R>(r2, (R)(0.5 * N));
-      const R rN = rpow<R>(r2, (R)(1.0 * N));
-      const R c = cos((R)N * theta), s = sin((R)N * theta);
-      const R norm1mzN = (R)1 - (R)2 * c * rN2 + rN;
-      const R denom = sqrt(norm1mzN);
-      if (denom != (R)0 && r2 != (R)0) {
-        const R pref = (R)2 * mpi2 * (R)N * sqrt(norm1mzN) * rpow<R>(r2, (R)(-1.0 + 0.5 * N)) * ((R)-1 + m3) / denom;
-        g0 += pref * (s * m2 + m1 * (c - rN2));
-        g1 += -pref * (s * m1 + m2 * (-c + rN2));
+      // broken potential: transcendental, evaluated site by site
+      using S = typename ScalarOf<R>::type;
+#pragma unroll
+      for (int l = 0; l < Lanes<R>::N; ++l) {
+        S a0 = Lanes<R>::get(g0, l), a1 = Lanes<R>::get(g1, l), a2 = Lanes<R>::get(g2, l);
+        broken<S>(Lanes<R>::get(m1, l), Lanes<R>::get(m2, l), Lanes<R>::get(m3, l), phys_k<S>(P, 2), P.k[8],
+                  a0, a1, a2);
+        Lanes<R>::set(g0, l, a0);
+        Lanes<R>::set(g1, l, a1);
+        Lanes<R>::set(g2, l, a2);
       }
-      g2 -= mpi2 * norm1mzN;
     }
     if (P.k[7]) g2 -= (R)2 * mpi2 * m3;
     g[0] = g0; g[1] = g1; g[2] = g2;
@@ -285,15 +321,18 @@ struct GinzburgLandau {
   static constexpr int NF = 4, NMAG = 0;
   static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true;
 
+  // derived slot: c[4] Lambda / 2
+  static void derive(Phys& P) { P.c[4] = 0.5 * P.c[1]; }
+
   // do_gradient_step_point, kernels.py:343-419
   template <typename R>
   __device__ static inline void gradient(const Jet<R, NF>& J, const Phys& P, R g[NF]) {
-    const R q = (R)P.c[0], lam = (R)P.c[1], u1 = (R)P.c[2];
+    const R q = pk<R>(P, 0), u1 = pk<R>(P, 2);
     const R A1 = J.f[0], A2 = J.f[1], psi1 = J.f[2], psi2 = J.f[3];
     const R psi_sq = psi1 * psi1 + psi2 * psi2;
     const R dA1dx = J.dx[0], dA1dy = J.dy[0], dA2dx = J.dx[1], dA2dy = J.dy[1];
     const R dpsi1dx = J.dx[2], dpsi1dy = J.dy[2], dpsi2dx = J.dx[3], dpsi2dy = J.dy[3];
-    const R pot = lam / (R)2 * (u1 * u1 - psi_sq);
+    const R pot = pk<R>(P, 4) * (u1 * u1 - psi_sq);
     const R Asq = A1 * A1 + A2 * A2;
     (void)dA2dx;
     (void)dA1dy;
@@ -349,21 +388,35 @@ struct Anisotropic {
   static constexpr int NF = 6, NMAG = 0;
   static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true;
 
+  template <typename R>
+  __device__ static inline R gamR(int i, int a, int b, const Phys& P) {
+    if (a == 0 && b == 0) return pk<R>(P, 13);
+    if (a == 1 && b == 1) return pk<R>(P, 14);
+    return i == 0 ? -pk<R>(P, 15) : pk<R>(P, 15);
+  }
   __device__ static inline double gam(int i, int a, int b, const Phys& P) {
     if (a == 0 && b == 0) return 2.0 * P.c[8];
     if (a == 1 && b == 1) return 2.0 * P.c[9];
     return (i == 0 ? -2.0 : 2.0) * P.c[10];
   }
 
+  // derived slots: c[12] kappa^2, c[13..15] 2 gamma1, 2 gamma2, 2 gamma12
+  static void derive(Phys& P) {
+    P.c[12] = P.c[0] * P.c[0];
+    P.c[13] = 2.0 * P.c[8];
+    P.c[14] = 2.0 * P.c[9];
+    P.c[15] = 2.0 * P.c[10];
+  }
+
   // do_gradient_step_point, kernels.py:556-658
   template <typename R>
   __device__ static inline void gradient(const Jet<R, NF>& J, const Phys& P, R g[NF]) {
-    const R kappa = (R)P.c[0], Q = (R)P.c[1];
-    const R a1 = (R)P.c[2], a2 = (R)P.c[3];
-    const R b1 = (R)P.c[4], b2 = (R)P.c[5], b3 = (R)P.c[6], b4 = (R)P.c[7];
+    const R Q = pk<R>(P, 1);
+    const R a1 = pk<R>(P, 2), a2 = pk<R>(P, 3);
+    const R b1 = pk<R>(P, 4), b2 = pk<R>(P, 5), b3 = pk<R>(P, 6), b4 = pk<R>(P, 7);
     const R A[2] = {J.f[0], J.f[1]};
     const R p1r = J.f[2], p1i = J.f[3], p2r = J.f[4], p2i = J.f[5];
-    const R k2 = kappa * kappa;
+    const R k2 = pk<R>(P, 12);
     // second derivative d_i d_j of component a
     auto d2 = [&](int i, int j, int a) -> R { return i != j ? J.dxy[a] : (i == 0 ? J.dxx[a] : J.dyy[a]); };
     auto d1 = [&](int i, int a) -> R { return i == 0 ? J.dx[a] : J.dy[a]; };
@@ -375,8 +428,8 @@ struct Anisotropic {
         R val = k2 * (d2(j, k, k) - d2(k, k, j));
         if (k == j) {
           const R Ak = A[k];
-          const R g00 = (R)gam(k, 0, 0, P), g01 = (R)gam(k, 0, 1, P), g10 = (R)gam(k, 1, 0, P),
-                  g11 = (R)gam(k, 1, 1, P);
+          const R g00 = gamR<R>(k, 0, 0, P), g01 = gamR<R>(k, 0, 1, P), g10 = gamR<R>(k, 1, 0, P),
+                  g11 = gamR<R>(k, 1, 1, P);
           val -= Q * g00 * (p1i * d1(k, 2) - p1r * d1(k, 3) - Q * Ak * (p1r * p1r + p1i * p1i));
           val -= Q * g01 * (p2i * d1(k, 2) - p2r * d1(k, 3) - Q * Ak * (p1r * p2r + p1i * p2i));
           val -= Q * g10 * (p1i * d1(k, 4) - p1r * d1(k, 5) - Q * Ak * (p2r * p1r + p2i * p1i));
@@ -397,8 +450,8 @@ struct Anisotropic {
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
       const R Ai = A[i];
-      const R g00 = (R)gam(i, 0, 0, P), g01 = (R)gam(i, 0, 1, P), g10 = (R)gam(i, 1, 0, P),
-              g11 = (R)gam(i, 1, 1, P);
+      const R g00 = gamR<R>(i, 0, 0, P), g01 = gamR<R>(i, 0, 1, P), g10 = gamR<R>(i, 1, 0, P),
+              g11 = gamR<R>(i, 1, 1, P);
       const R dAii = d1(i, i);
       const R QQAA = Q * Q * Ai * Ai;
       EG[2] -= g00 * (d2(i, i, 2) - QQAA * p1r - Q * (p1i * dAii + Ai * d1(i, 3) + Ai * d1(i, 3)));
