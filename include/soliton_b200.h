@@ -115,6 +115,13 @@ int ss_tma_enabled(const ss_handle *h);
 int ss_autotune(ss_handle *h, int iters, float *ms_out);
 /* Variant chosen for a flow mode (0..5): 1 pipelined, 0 one tile per CTA, -1 bad args. */
 int ss_get_variant(const ss_handle *h, int mode);
+/* Failure-detection hook.  Sets the bound (clock64 cycles, default 2e9) of every
+ * device-side mbarrier wait of this handle's kernels; with inject != 0 the next
+ * TMA-staged stage kernel's barrier expects 16 bytes more than its loads deliver,
+ * so its bounded wait expires: the kernel records SS_ERR_TIMEOUT, waits the bound
+ * again for its own copies and returns without computing.  No fault, trap or
+ * unbounded spin is involved; after SS_ERR_TIMEOUT re-bind the handle. */
+int ss_debug_wait_timeout(ss_handle *h, long long wait_cycles, int inject);
 
 /* One gradient evaluation of an arbitrary field buffer: energy_gradient (nullable)
  * receives the theory's projected dE/dphi, l_out (nullable) receives -dt*dE/dphi.

@@ -58,6 +58,10 @@ class NonFiniteError(SolverError):
     """A reduction produced NaN or Inf (SS_ERR_NONFINITE)."""
 
 
+class DeviceTimeoutError(SolverError):
+    """A bounded device-side wait expired (SS_ERR_TIMEOUT); re-bind before further use."""
+
+
 _lib = None
 
 _P = ctypes.c_void_p
@@ -77,6 +81,7 @@ _SIG = {
     "ss_tma_enabled": ([_P], _I),
     "ss_autotune": ([_P, _I, _P], _I),
     "ss_get_variant": ([_P, _I], _I),
+    "ss_debug_wait_timeout": ([_P, ctypes.c_longlong, _I], _I),
     "ss_gradient": ([_P, _P, _P, _P], _I),
     "ss_energy_density": ([_P, _P, _P], _I),
     "ss_energy": ([_P, _P, ctypes.POINTER(_D)], _I),
@@ -119,6 +124,8 @@ def check(status: int):
         raise ValueError(msg)
     if status == SS_ERR_NONFINITE:
         raise NonFiniteError(status, msg)
+    if status == SS_ERR_TIMEOUT:
+        raise DeviceTimeoutError(status, msg)
     raise SolverError(status, msg)
 
 

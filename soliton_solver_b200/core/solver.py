@@ -130,6 +130,15 @@ class Solver:
         return {m: (float(ms[2 * m]), float(ms[2 * m + 1]), int(self._lib.ss_get_variant(self._h, m)))
                 for m in (1, 2, 3, 4)}
 
+    def debug_wait_timeout(self, wait_cycles: int, inject: bool):
+        """Failure-detection hook: bound of the device waits; optionally make the next
+        stage kernel's wait expire (see ss_debug_wait_timeout)."""
+        nat.check(self._lib.ss_debug_wait_timeout(self._h, int(wait_cycles), 1 if inject else 0))
+
+    def rebind(self):
+        """Re-bind the current buffers (resets the device step state)."""
+        self._bind(self.field, self.velocity)
+
     def check_status(self):
         nat.check(self._lib.ss_check_status(self._h))
 

@@ -115,6 +115,8 @@ struct ss_handle {
   // per flow mode: 1 = persistent pipelined kernel, 0 = one tile per CTA (autotuned)
   int use_pipe[6] = {1, 1, 1, 1, 1, 1};
   float tune_ms[6][2] = {};
+  long long wait_cycles = WAIT_CYCLES;
+  mutable int inject_timeout = 0;  // test hook, consumed by the next flow launch
 };
 
 namespace {
@@ -302,13 +304,10 @@ struct Fused {
   // tma: use the TMA-staged instantiation (A.tm_* must describe A's buffers)
   static inline unsigned long long smem_done[2][6] = {};
 
-  // dynamic shared memory of flow_kernel: the staged buffers, plus (FP32 energy
-  // stages) room for the FP64 copy of the tile after the first buffer
+  // dynamic shared memory of flow_kernel: the staged buffers
   template <bool TMA_, int MODE>
   static constexpr size_t flow_smem() {
-    const size_t staged = TMA_ ? flow_buffers(MODE) * BUF : BUF;
-    const size_t energy = (sizeof(R) == 4 && (MODE == M_S1 || MODE == M_ENERGY)) ? BUF + 2 * BUF : 0;
-    return staged > energy ? staged : energy;
+    return TMA_ ? flow_buffers(MODE) * BUF : BUF;
   }
 
   template <bool TMA_, int MODE>
@@ -378,7 +377,12 @@ struct Fused {
   }
 
   // tma: use the TMA-staged instantiations (A.tm_* must describe A's buffers)
-  static int launch(const ss_handle* h, const FlowArgs<R>& A, bool tma) {
+  static int launch(const ss_handle* h, const FlowArgs<R>& A0, bool tma) {
+    FlowArgs<R> A = A0;
+    if (h->inject_timeout && tma) {
+      A.tx_extra = 16;
+      h->inject_timeout = 0;
+    }
     if (!tma) return launch_tma<false>(h, A);
     if (!h->use_pipe[A.mode]) return launch_tma<true>(h, A);
     switch (A.mode) {
@@ -395,6 +399,7 @@ struct Fused {
   static FlowArgs<R> base_args(const ss_handle* h) {
     FlowArgs<R> A;
     memset(&A, 0, sizeof(A));
+    A.wait_cycles = h->wait_cycles;
     A.G = h->G;
     A.P = h->P;
     A.st = h->st;
@@ -859,6 +864,14 @@ int ss_autotune(ss_handle* h, int iters, float* ms_out) {
       ms_out[2 * m + 1] = h->tune_ms[m][1];
     }
   return take_status(h);
+}
+
+int ss_debug_wait_timeout(ss_handle* h, long long wait_cycles, int inject) {
+  if (!h) return fail(SS_ERR_ARG, "NULL handle");
+  if (wait_cycles <= 0) return fail(SS_ERR_ARG, "wait_cycles must be positive");
+  h->wait_cycles = wait_cycles;
+  h->inject_timeout = inject ? 1 : 0;
+  return SS_OK;
 }
 
 int ss_get_variant(const ss_handle* h, int mode) {

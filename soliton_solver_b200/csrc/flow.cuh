@@ -30,7 +30,7 @@ namespace ssb {
 enum FlowMode { M_GRAD = 0, M_S1 = 1, M_S2 = 2, M_S3 = 3, M_S4 = 4, M_ENERGY = 5 };
 enum { ST_TIMEOUT = 6 };
 
-// Upper bound of a device-side wait on an mbarrier (~1 s at 1.9 GHz).  On expiry
+// Default bound of a device-side wait on an mbarrier (~1 s at 1.9 GHz).  On expiry
 // the kernel records ST_TIMEOUT, waits the same bound again for its copies in
 // flight and returns without computing.
 constexpr long long WAIT_CYCLES = 2000000000LL;
@@ -62,6 +62,8 @@ struct FlowArgs {
   int arrest_update;  // after the energy: arrest = killkinen && E > E_last; E_last = E
   int init_state;     // first S1 of a call: arrest = 0 and (unless NaN) E_last = prev_energy
   double prev_energy;
+  long long wait_cycles;  // bound of every mbarrier wait (clock64 cycles)
+  unsigned tx_extra;      // test hook: bytes the barrier expects beyond what is loaded (normally 0)
   Grid G;
   Phys P;
 };
@@ -117,11 +119,11 @@ __device__ inline void tma_load_3d(void* dst, const CUtensorMap* map, int c0, in
       ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
       : "memory");
 }
-// Bounded wait; returns false when WAIT_CYCLES elapsed first.
-__device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Bounded wait; returns false when `limit` clock64 cycles elapsed first.
+__device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit) {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > WAIT_CYCLES) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
 }
@@ -472,15 +474,15 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
     __syncthreads();
     if (threadIdx.x == 0) {
       const uint32_t bytes = (uint32_t)(sizeof(R) * BUF) * (1u + (need_v ? 1u : 0u) + (need_l ? 1u : 0u));
-      mbar_expect_tx(&bar, bytes);
+      mbar_expect_tx(&bar, bytes + A.tx_extra);
       tma_load_3d(B0, &A.tm_phi, y0 - TS::YOFF, x0 - 2, 0, &bar);
       if (need_v) tma_load_3d(B1, &A.tm_vel, y0 - TS::YOFF, x0 - 2, 0, &bar);
       if (need_l) tma_load_3d(B2, &A.tm_l, y0 - TS::YOFF, x0 - 2, 0, &bar);
     }
-    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0));
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0, A.wait_cycles));
     if (!ok) {
       if (threadIdx.x == 0) atomicExch(&st->status, (int)ST_TIMEOUT);
-      mbar_wait_bounded(&bar, 0);
+      mbar_wait_bounded(&bar, 0, A.wait_cycles);
       return;
     }
     if (mode == M_S2 || mode == M_S3 || mode == M_S4) {
@@ -536,21 +538,7 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
   }
   if constexpr (MODE == M_S1 || MODE == M_ENERGY) {
     if (do_energy) {
-      if constexpr (sizeof(R) == 4) {
-        // convert the staged FP32 tile to FP64 once (each value then serves all the
-        // stencils it enters without further conversions); placed after B0
-        double* Td = reinterpret_cast<double*>(B1);
-        for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
-          const float4 v = *reinterpret_cast<const float4*>(T + i);
-          *reinterpret_cast<double2*>(Td + i) = make_double2((double)v.x, (double)v.y);
-          *reinterpret_cast<double2*>(Td + i + 2) = make_double2((double)v.z, (double)v.w);
-        }
-        __syncthreads();
-        if (fast)
-          e_acc = energy_tile<TH, R, TX, TY, NT, true, double>(A, Td, x0, y0);
-        else
-          e_acc = energy_tile<TH, R, TX, TY, NT, false, double>(A, Td, x0, y0);
-      } else {
+      {
         if (fast)
           e_acc = energy_tile<TH, R, TX, TY, NT, true>(A, T, x0, y0);
         else
@@ -653,7 +641,7 @@ __global__ void __launch_bounds__(NT, 1) flow_kernel_pipe(const __grid_constant_
   auto issue = [&](int slot, int tile) {
     R* base = ring + slot * SLOT;
     const int x0 = (tile / tiles_y) * TX, y0 = (tile % tiles_y) * TY;
-    mbar_expect_tx(&full[slot], bytes);
+    mbar_expect_tx(&full[slot], bytes + A.tx_extra);
     tma_load_3d(base, &A.tm_phi, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
     if (need_v) tma_load_3d(base + BUF, &A.tm_vel, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
     if (need_l) tma_load_3d(base + 2 * BUF, &A.tm_l, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
@@ -683,13 +671,14 @@ __global__ void __launch_bounds__(NT, 1) flow_kernel_pipe(const __grid_constant_
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
     const int slot = k % STAGES;
     const uint32_t parity = (uint32_t)((k / STAGES) & 1);
-    const bool ok = __syncthreads_and(mbar_wait_bounded(&full[slot], parity));
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&full[slot], parity, A.wait_cycles));
     if (!ok) {
       // record, then wait (bounded) for every load still in flight before leaving
       if (threadIdx.x == 0) atomicExch(&st->status, (int)ST_TIMEOUT);
       for (int s = 0; s < STAGES; ++s) {
         const int kk = k + s;
-        if (blockIdx.x + kk * gridDim.x < ntiles) mbar_wait_bounded(&full[kk % STAGES], (uint32_t)((kk / STAGES) & 1));
+        if (blockIdx.x + kk * gridDim.x < ntiles)
+          mbar_wait_bounded(&full[kk % STAGES], (uint32_t)((kk / STAGES) & 1), A.wait_cycles);
       }
       return;
     }

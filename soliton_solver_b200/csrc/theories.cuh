@@ -49,11 +49,12 @@ struct ChiralMagnet {
   // term is one fused multiply-add; R is a scalar or a packed pair of sites.
   // derived slots filled on the host (ChiralMagnet::derive):
   //   c[12] -2 D10  c[13] -2 D11  c[14] 2 D00  c[15] 2 D01  c[16] 2 D10  c[17] 2 D11
-  //   c[18] -2 D00  c[19] -2 D01  c[20] -2 coup_K
+  //   c[18] -2 D00  c[19] -2 D01  c[20] -2 coup_K  c[21] 1/(2 coup_mu)
   static void derive(Phys& P) {
     P.c[12] = -2.0 * P.c[5]; P.c[13] = -2.0 * P.c[6]; P.c[14] = 2.0 * P.c[3]; P.c[15] = 2.0 * P.c[4];
     P.c[16] = 2.0 * P.c[5]; P.c[17] = 2.0 * P.c[6]; P.c[18] = -2.0 * P.c[3]; P.c[19] = -2.0 * P.c[4];
     P.c[20] = -2.0 * P.c[0];
+    P.c[21] = P.c[2] != 0.0 ? 1.0 / (2.0 * P.c[2]) : 0.0;
   }
   template <typename R>
   __device__ static inline void gradient(const Jet<R, NF>& J, const Phys& P, R g[NF]) {
@@ -85,7 +86,7 @@ struct ChiralMagnet {
 
   // compute_energy_point, kernels.py:125-216
   __device__ static inline double energy(const Jet1<double, NF>& J, const Phys& P, double dA) {
-    const double cK = P.c[0], ch = P.c[1], cmu = P.c[2];
+    const double cK = P.c[0], ch = P.c[1];
     const double D00 = P.c[3], D01 = P.c[4], D10 = P.c[5], D11 = P.c[6];
     double e = 0.0;
 #pragma unroll
@@ -97,11 +98,12 @@ struct ChiralMagnet {
     // i = x
     if (D00 != 0.0) { e += D00 * m[1] * J.dx[2]; e -= D00 * m[2] * J.dx[1]; }
     if (D10 != 0.0) { e -= D10 * m[0] * J.dx[2]; e += D10 * m[2] * J.dx[0]; }
-    if (P.k[0]) e -= m[3] * J.dx[0] + J.dx[3] * J.dx[3] / (2.0 * cmu);
+    const double i2mu = P.c[21];  // 1 / (2 coup_mu), precomputed on the host
+    if (P.k[0]) e -= m[3] * J.dx[0] + J.dx[3] * J.dx[3] * i2mu;
     // i = y
     if (D01 != 0.0) { e += D01 * m[1] * J.dy[2]; e -= D01 * m[2] * J.dy[1]; }
     if (D11 != 0.0) { e -= D11 * m[0] * J.dy[2]; e += D11 * m[2] * J.dy[0]; }
-    if (P.k[0]) e -= m[3] * J.dy[1] + J.dy[3] * J.dy[3] / (2.0 * cmu);
+    if (P.k[0]) e -= m[3] * J.dy[1] + J.dy[3] * J.dy[3] * i2mu;
     const double mz = m[2];
     e += ch * (1.0 - mz);
     e += cK * (1.0 - mz * mz);

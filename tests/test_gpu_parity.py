@@ -345,3 +345,30 @@ def test_coupling_partials_vs_finite_differences(case, prec):
             pass  # Lambda enters the energy directly
         want = (ref.energy(th, Fo, p_i, pp) - ref.energy(th, Fo, p_i, pm)) / (2 * h)
         assert abs(got - want) <= 1e-6 * max(1.0, abs(want)), (name, got, want)
+
+
+def test_bounded_wait_timeout_is_reported_and_recoverable():
+    """A stage kernel whose mbarrier can never complete (the test hook makes it expect
+    16 bytes nobody sends) gives up after its bounded wait: status SS_ERR_TIMEOUT,
+    no fault, and the handle works again after a re-bind."""
+    from soliton_solver_b200._native import DeviceTimeoutError
+    theory = load_theory("Chiral magnet")
+    rp = theory.params.default_params(xlen=40, ylen=64, xsize=2.0, ysize=3.2, dmi_term="Heusler",
+                                      unit_magnetization=True).resolved()
+    p_i, p_f = theory.params.pack_device_params(rp)
+    s = Solver(0, p_i, p_f, "fp32")
+    F = _smooth_field("chiral_magnet", rp, 9)
+    f, v = _dev(F, "fp32"), _dev(np.zeros_like(F), "fp32")
+    s.bind(f, v)
+    assert s.tma_enabled
+    s.debug_wait_timeout(2_000_000, inject=True)   # about a millisecond
+    eg = torch.empty_like(f)
+    s.gradient(f, eg, None)
+    with pytest.raises(DeviceTimeoutError):
+        s.check_status()
+    s.debug_wait_timeout(2_000_000_000, inject=False)
+    s.rebind()
+    s.gradient(f, eg, None)
+    s.check_status()
+    _, eg_w = ref.gradient_step("chiral_magnet", ref.as_field(_cast(F, "fp32"), p_i), p_i, p_f)
+    _cmp(eg.cpu().numpy(), eg_w, "fp32", "gradient after recovery")
