@@ -88,6 +88,7 @@ _SIG = {
     "ss_charge_density": ([_P, _P, _I, _P], _I),
     "ss_charge": ([_P, _P, _I, ctypes.POINTER(_D)], _I),
     "ss_coupling_grad": ([_P, _P, _I, ctypes.POINTER(_D)], _I),
+    "ss_energy_noalloc": ([_I, _P, _I, _P, _I, _I, _P, ctypes.POINTER(_D), _P], _I),
     "ss_rk4_stage": ([_P, _P, _P, _P, _P, _P, _P, _D], _I),
     "ss_rk4_finalize": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
 }

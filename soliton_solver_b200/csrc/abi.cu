@@ -1027,3 +1027,87 @@ int ss_rk4_finalize(ss_handle* h, void* velocity, void* field, const void* k1, c
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Total energy without any allocation.
+//
+// Some callers cannot allocate device memory at the point where they need an
+// energy: code that runs while a stream is being captured into a CUDA graph
+// (cudaMalloc is not allowed there), hosts whose memory manager owns the whole
+// device and forbids further allocations, and interactive loops that must not
+// call cudaMalloc because it synchronises the device.  For them
+// ss_energy_noalloc keeps its scratch (the per-block partial sums and the
+// reduction state) in the file-scope array below, which every GPU that loads
+// this library holds until exit.
+// ===========================================================================
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = 512 * 1024;   // 256 B state + up to 65504 block partials
+__device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+void* g_noalloc_addr[64] = {};                          // device address of the array, per device
+
+// Device address of the static scratch on the current device (looked up once per device).
+int noalloc_scratch(void** out) {
+  int dev = -1;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SS_ERR_ARG, "device ordinal %d out of range", dev);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return SS_OK;
+}
+
+}  // namespace
+
+extern "C" int ss_energy_noalloc(int theory, const int32_t* p_i, int n_i, const double* p_f, int n_f,
+                                 int precision, const void* field, double* out, void* stream) {
+  if (!field || !out) return fail(SS_ERR_ARG, "field and out must not be NULL");
+  if (precision != SS_FP32 && precision != SS_FP64)
+    return fail(SS_ERR_ARG, "ss_energy_noalloc supports SS_FP32 and SS_FP64 fields");
+  ss_handle h;  // on the stack: decoding the parameters allocates nothing
+  h.theory = theory;
+  h.precision = precision;
+  int rc = decode(&h, theory, p_i, n_i, p_f, n_f);
+  if (rc) return rc;
+  h.elem = precision == SS_FP32 ? 4 : 8;
+  const long long tiles = (long long)((h.G.X + TX - 1) / TX) * ((h.G.Y + TY - 1) / TY);
+  const size_t need = 256 + (size_t)tiles * sizeof(double);
+  if (need > NOALLOC_SCRATCH_BYTES)
+    return fail(SS_ERR_ARG,
+                "lattice of %lld tiles (16 x 64 sites each) needs %zu bytes of scratch; the allocation-free "
+                "entry point holds %zu (at most %zu tiles)",
+                tiles, need, NOALLOC_SCRATCH_BYTES, (NOALLOC_SCRATCH_BYTES - 256) / sizeof(double));
+  h.nblocks = (int)tiles;
+  h.stream = (cudaStream_t)stream;
+  void* scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  h.st = (StepState*)scratch;
+  h.partial = (double*)((char*)scratch + 256);
+  // the last call's contents stay in the array: the reduction state must start at zero
+  CK(cudaMemsetAsync(h.st, 0, sizeof(StepState), h.stream));
+  rc = dispatch(&h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (precision == SS_FP32) {
+      FlowArgs<float> A = Fused<TH, float>::base_args(&h);
+      A.mode = M_ENERGY;
+      A.phi = (const float*)field;
+      A.with_energy = 1;
+      return Fused<TH, float>::template launch_mode<false, M_ENERGY>(&h, A);
+    }
+    FlowArgs<double> A = Fused<TH, double>::base_args(&h);
+    A.mode = M_ENERGY;
+    A.phi = (const double*)field;
+    A.with_energy = 1;
+    return Fused<TH, double>::template launch_mode<false, M_ENERGY>(&h, A);
+  });
+  if (rc) return rc;
+  StepState s;
+  CK(cudaMemcpyAsync(&s, h.st, sizeof(StepState), cudaMemcpyDeviceToHost, h.stream));
+  CK(cudaStreamSynchronize(h.stream));
+  *out = s.scalar;
+  if (s.status) return fail(SS_ERR_NONFINITE, "the energy reduction produced a non-finite value");
+  return SS_OK;
+}
