@@ -128,6 +128,13 @@ int ss_debug_wait_timeout(ss_handle *h, long long wait_cycles, int inject);
  * Replaces theory.kernels.do_gradient_step_kernel(l_out, Field, d1, d2, EG, p_i, p_f)
  * (core/integrator.py:15-48 with e.g. theories/chiral_magnet/kernels.py:398-511). */
 int ss_gradient(ss_handle *h, const void *field, void *energy_gradient, void *l_out);
+/* Functional derivative dE/dphi of the energy density at every site (element type
+ * of the handle): the same stencil as the flow's gradient but without the unit-norm
+ * projection and without the chiral magnet's halo zeroing, and with the demag psi
+ * row converted from the flow's -coup_mu dE/dpsi to dE/dpsi.  dA times this is the
+ * gradient of the total energy up to O(h^4) and boundary terms; it is the backward
+ * of the autograd energy.  No reference counterpart (new capability). */
+int ss_energy_gradient(ss_handle *h, const void *field, void *grad);
 /* Per-site energy x dA (double).  Replaces compute_energy_kernel
  * (e.g. theories/chiral_magnet/kernels.py:219-251). */
 int ss_energy_density(ss_handle *h, const void *field, double *density);

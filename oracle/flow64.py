@@ -227,8 +227,11 @@ def chiral_energy_density(F, d1, p_i, p_f):
     return e * dA
 
 
-def chiral_gradient(F, d1, d2, p_i, p_f):
-    """Projected energy gradient, chiral_magnet/kernels.py:398-511 (before the l = -dt EG write)."""
+def chiral_gradient(F, d1, d2, p_i, p_f, raw=False):
+    """Projected energy gradient, chiral_magnet/kernels.py:398-511 (before the l = -dt EG write).
+
+    raw=True skips the halo zeroing and the projection and returns dE/dpsi for the
+    demag row (the flow stores -coup_mu * dE/dpsi there)."""
     nf, X, Y = F.shape
     h = int(p_i[2])
     cK, ch, cmu = float(p_f[6]), float(p_f[7]), float(p_f[8])
@@ -261,6 +264,10 @@ def chiral_gradient(F, d1, d2, p_i, p_f):
         for i in range(nc):
             EG[i] = EG[i] + d1[i, 3]
             EG[3] = EG[3] + (cmu * d1[i, i] - d2[i, i, 3])
+    if raw:
+        if demag:
+            EG[3] = EG[3] * (-1.0 / cmu)
+        return EG
     mask = _halo_mask(X, Y, h)
     EG[:, mask] = 0.0
     return project_orthogonal(EG, F, nmag)
@@ -334,8 +341,9 @@ def baby_skyrme_energy_density(F, d1, p_i, p_f):
     return e * dA
 
 
-def baby_skyrme_gradient(F, d1, d2, p_i, p_f):
-    """Projected gradient, baby_skyrme/kernels.py:308-458 (no halo zeroing in this theory)."""
+def baby_skyrme_gradient(F, d1, d2, p_i, p_f, raw=False):
+    """Projected gradient, baby_skyrme/kernels.py:308-458 (no halo zeroing in this theory);
+    raw=True skips the projection."""
     mpi = float(p_f[6]); mpi2 = mpi * mpi
     kappa = float(p_f[7]); kappa2 = kappa * kappa
     N = int(p_i[19])
@@ -417,6 +425,8 @@ def baby_skyrme_gradient(F, d1, d2, p_i, p_f):
     if p_i[18]:
         g2 = g2 - 2.0 * mpi2 * m3
     EG = np.stack([g0, g1, g2])
+    if raw:
+        return EG
     return project_orthogonal(EG, F, int(p_i[10]))
 
 
@@ -631,6 +641,16 @@ def gradient_step(theory, F, p_i, p_f):
     d2 = second_derivatives(F, p_i, p_f)
     EG = _GRAD[theory](F, d1, d2, p_i, p_f)
     return -float(p_f[5]) * EG, EG
+
+
+def raw_gradient(theory, F, p_i, p_f):
+    """Unprojected functional derivative dE/dphi (the flow's stencil without projection or
+    halo zeroing; true dE/dpsi for the chiral demag row)."""
+    d1 = first_derivatives(F, p_i, p_f)
+    d2 = second_derivatives(F, p_i, p_f)
+    if theory in ("chiral_magnet", "baby_skyrme"):
+        return _GRAD[theory](F, d1, d2, p_i, p_f, raw=True)
+    return _GRAD[theory](F, d1, d2, p_i, p_f)
 
 
 def energy_density(theory, F, p_i, p_f):

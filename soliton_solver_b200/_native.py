@@ -83,6 +83,7 @@ _SIG = {
     "ss_get_variant": ([_P, _I], _I),
     "ss_debug_wait_timeout": ([_P, ctypes.c_longlong, _I], _I),
     "ss_gradient": ([_P, _P, _P, _P], _I),
+    "ss_energy_gradient": ([_P, _P, _P], _I),
     "ss_energy_density": ([_P, _P, _P], _I),
     "ss_energy": ([_P, _P, ctypes.POINTER(_D)], _I),
     "ss_charge_density": ([_P, _P, _I, _P], _I),

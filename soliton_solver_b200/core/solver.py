@@ -150,6 +150,15 @@ class Solver:
         with torch.cuda.device(self.device):
             nat.check(self._lib.ss_gradient(self._h, _ptr(field), _ptr(energy_gradient), _ptr(l_out)))
 
+    def energy_gradient(self, field, out=None):
+        """dE/dphi per site (unprojected; see ss_energy_gradient)."""
+        self._check(field)
+        out = out if out is not None else torch.empty_like(field)
+        self._check(out)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_energy_gradient(self._h, _ptr(field), _ptr(out)))
+        return out
+
     def energy(self, field) -> float:
         self._check(field)
         out = ctypes.c_double()

@@ -547,9 +547,10 @@ struct Fused {
     return rc;
   }
 
-  static int gradient(ss_handle* h, const void* field, void* eg, void* l_out) {
+  static int gradient(ss_handle* h, const void* field, void* eg, void* l_out, int raw = 0) {
     FlowArgs<R> A = base_args(h);
     A.mode = M_GRAD;
+    A.grad_raw = raw;
     A.phi = (const R*)field;
     A.out_eg = (R*)eg;
     A.out_l = (R*)l_out;
@@ -940,6 +941,18 @@ int ss_gradient(ss_handle* h, const void* field, void* energy_gradient, void* l_
     using TH = std::remove_pointer_t<decltype(tag)>;
     if (h->precision == SS_FP32) return Fused<TH, float>::gradient(h, field, energy_gradient, l_out);
     return Fused<TH, double>::gradient(h, field, energy_gradient, l_out);
+  });
+}
+
+int ss_energy_gradient(ss_handle* h, const void* field, void* grad) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!field || !grad) return fail(SS_ERR_ARG, "NULL argument");
+  if (h->precision == SS_PLAIN_FP64) return fail(SS_ERR_ARG, "ss_energy_gradient needs SS_FP32 or SS_FP64");
+  return dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (h->precision == SS_FP32) return Fused<TH, float>::gradient(h, field, grad, nullptr, 1);
+    return Fused<TH, double>::gradient(h, field, grad, nullptr, 1);
   });
 }
 

@@ -62,6 +62,7 @@ struct FlowArgs {
   int arrest_update;  // after the energy: arrest = killkinen && E > E_last; E_last = E
   int init_state;     // first S1 of a call: arrest = 0 and (unless NaN) E_last = prev_energy
   double prev_energy;
+  int grad_raw;           // M_GRAD: unprojected, not halo-zeroed dE/dphi with true saddle rows
   long long wait_cycles;  // bound of every mbarrier wait (clock64 cycles)
   unsigned tx_extra;      // test hook: bytes the barrier expects beyond what is loaded (normally 0)
   Grid G;
@@ -307,6 +308,18 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
 
     V g[NF];
     TH::gradient(J, A.P, g);
+    if constexpr (MODE == M_GRAD) {
+      if (A.grad_raw) {
+        // functional derivative of the energy: no halo zeroing, no projection, and
+        // rows the flow stores scaled (saddle fields) converted to dE/dphi
+        TH::true_rows(g, A.P);
+#pragma unroll
+        for (int a = 0; a < NF; ++a) {
+          if (A.out_eg) gstore<V, R>(A.out_eg + a * N + sidx, g[a], FAST, v1);
+        }
+        continue;
+      }
+    }
     if (TH::HALO_ZERO && !FAST) {
       const bool e0 = gx < G.halo || gx > G.X - G.halo - 1 || gy < G.halo || gy > G.Y - G.halo - 1;
       const bool e1 = gx < G.halo || gx > G.X - G.halo - 1 || gy + 1 < G.halo || gy + 1 > G.Y - G.halo - 1;

@@ -49,12 +49,13 @@ struct ChiralMagnet {
   // term is one fused multiply-add; R is a scalar or a packed pair of sites.
   // derived slots filled on the host (ChiralMagnet::derive):
   //   c[12] -2 D10  c[13] -2 D11  c[14] 2 D00  c[15] 2 D01  c[16] 2 D10  c[17] 2 D11
-  //   c[18] -2 D00  c[19] -2 D01  c[20] -2 coup_K  c[21] 1/(2 coup_mu)
+  //   c[18] -2 D00  c[19] -2 D01  c[20] -2 coup_K  c[21] 1/(2 coup_mu)  c[22] -1/coup_mu
   static void derive(Phys& P) {
     P.c[12] = -2.0 * P.c[5]; P.c[13] = -2.0 * P.c[6]; P.c[14] = 2.0 * P.c[3]; P.c[15] = 2.0 * P.c[4];
     P.c[16] = 2.0 * P.c[5]; P.c[17] = 2.0 * P.c[6]; P.c[18] = -2.0 * P.c[3]; P.c[19] = -2.0 * P.c[4];
     P.c[20] = -2.0 * P.c[0];
     P.c[21] = P.c[2] != 0.0 ? 1.0 / (2.0 * P.c[2]) : 0.0;
+    P.c[22] = P.c[2] != 0.0 ? -1.0 / P.c[2] : 0.0;
   }
   template <typename R>
   __device__ static inline void gradient(const Jet<R, NF>& J, const Phys& P, R g[NF]) {
@@ -82,6 +83,13 @@ struct ChiralMagnet {
       g[1] += J.dy[3];
       g[3] = vfma(cmu, J.dy[1], g[3]) - J.dyy[3];
     }
+  }
+
+  // The flow's psi row is -coup_mu * dE/dpsi (psi is maximised, kernels.py:498-503):
+  // dE/dpsi = -div m + lap(psi)/coup_mu = -row / coup_mu.
+  template <typename R>
+  __device__ static inline void true_rows(R g[NF], const Phys& P) {
+    if (P.k[0]) g[3] = g[3] * pk<R>(P, 22);
   }
 
   // compute_energy_point, kernels.py:125-216
@@ -142,6 +150,8 @@ struct ChiralMagnet {
 struct BabySkyrme {
   static constexpr int NF = 3, NMAG = 3;
   static constexpr bool CONSTRAINED = true, HALO_ZERO = false, NEED_XY = true;
+  template <typename R>
+  __device__ static inline void true_rows(R*, const Phys&) {}
 
   template <typename S>
   __device__ static inline S spow(S a, S b) {
@@ -322,6 +332,8 @@ struct BabySkyrme {
 struct GinzburgLandau {
   static constexpr int NF = 4, NMAG = 0;
   static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true;
+  template <typename R>
+  __device__ static inline void true_rows(R*, const Phys&) {}
 
   // derived slot: c[4] Lambda / 2
   static void derive(Phys& P) { P.c[4] = 0.5 * P.c[1]; }
@@ -389,6 +401,8 @@ struct GinzburgLandau {
 struct Anisotropic {
   static constexpr int NF = 6, NMAG = 0;
   static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true;
+  template <typename R>
+  __device__ static inline void true_rows(R*, const Phys&) {}
 
   template <typename R>
   __device__ static inline R gamR(int i, int a, int b, const Phys& P) {

@@ -82,3 +82,43 @@ def test_trajectories(path):
     np.testing.assert_allclose(err, g["err_traj"], rtol=1e-12, atol=1e-14)
     _close(F.reshape(-1), g["final_field"], 1e-12)
     _close(V.reshape(-1), g["final_velocity"], 1e-12)
+
+
+def _fd_vs_gradient(key, kw, comps):
+    from soliton_solver_b200.theories import load_theory
+    names = {"anisotropic_superconductor": "s+id superconductor", "ginzburg_landau_superconductor": "Abelian Higgs"}
+    th = load_theory(names[key])
+    rp = th.params.default_params(**kw).resolved()
+    p_i, p_f = th.params.pack_device_params(rp)
+    rng = np.random.default_rng(5)
+    X, Y, nf = rp.xlen, rp.ylen, rp.number_total_fields
+    x = np.linspace(-1, 1, X)[:, None]
+    y = np.linspace(-1, 1, Y)[None, :]
+    F = np.stack([0.3 * np.sin(2 * x + rng.normal()) * np.cos(1.5 * y + rng.normal()) for _ in range(nf)])
+    bump = (np.sin(np.pi * (x + 1) / 2) * np.sin(np.pi * (y + 1) / 2)) ** 8
+    g = ref.raw_gradient(key, F, p_i, p_f) * float(p_f[4])
+    out = []
+    for a in comps:
+        D = np.zeros_like(F)
+        D[a] = bump * np.cos(2 * x + y)
+        eps = 1e-5
+        fd = (ref.energy(key, F + eps * D, p_i, p_f) - ref.energy(key, F - eps * D, p_i, p_f)) / (2 * eps)
+        out.append((float((g * D).sum()), fd))
+    return out
+
+
+def test_splusid_condensate_rows_are_not_dE_dpsi():
+    """Pins a property of the reference: the s+id gradient rows of the condensates
+    (anisotropic_superconductor/kernels.py:617-650) are not the derivative of its
+    energy (kernels.py:97-170), while the gauge rows are (to O(h^4)).  The flow, the
+    kernels and the autograd backward follow the reference's rows."""
+    kw = dict(xlen=56, ylen=60, xsize=5.5, ysize=5.9)
+    gauge = _fd_vs_gradient("anisotropic_superconductor", kw, (0, 1))
+    for ad, fd in gauge:
+        assert abs(ad - fd) <= 1e-3 * abs(fd)
+    cond = _fd_vs_gradient("anisotropic_superconductor", kw, (2, 3, 4, 5))
+    assert all(abs(ad - fd) > 0.5 * abs(fd) for ad, fd in cond)
+    # the Abelian Higgs rows are all consistent
+    for ad, fd in _fd_vs_gradient("ginzburg_landau_superconductor", dict(xlen=64, ylen=68, xsize=6.3, ysize=6.7),
+                                  (0, 1, 2, 3)):
+        assert abs(ad - fd) <= 1e-3 * abs(fd)
