@@ -117,7 +117,8 @@ def test_splusid_condensate_rows_are_not_dE_dpsi():
     for ad, fd in gauge:
         assert abs(ad - fd) <= 1e-3 * abs(fd)
     cond = _fd_vs_gradient("anisotropic_superconductor", kw, (2, 3, 4, 5))
-    assert all(abs(ad - fd) > 0.5 * abs(fd) for ad, fd in cond)
+    assert all(abs(ad - fd) > 0.1 * abs(fd) for ad, fd in cond)   # off by 25% to 80x
+    assert any(abs(ad - fd) > 10 * abs(fd) for ad, fd in cond)
     # the Abelian Higgs rows are all consistent
     for ad, fd in _fd_vs_gradient("ginzburg_landau_superconductor", dict(xlen=64, ylen=68, xsize=6.3, ysize=6.7),
                                   (0, 1, 2, 3)):
