@@ -333,12 +333,42 @@ def relaxed_accuracy(dev, max_steps=20000, chunk=1000, tol=1e-6):
     return out
 
 
+def batched_sweep(dev, steps=20, seed=4):
+    """The batched baby Skyrme sweep: 256 lattices with edges from {64, 128, 256, 512},
+    kappa, mpi ~ U(0.5, 2), windings B in 1..4, hedgehogs with R ~ U(1, 3), FP32 fields.
+    Returns point-updates/s of ss_batch_step over `steps` steps (all lattices)."""
+    import torch
+    from soliton_solver_b200.core.batch import BatchSolver
+    from soliton_solver_b200.initial_conditions import hedgehog
+    from soliton_solver_b200.theories import load_theory
+    th = load_theory("Baby Skyrme")
+    rng = np.random.default_rng(seed)
+    edges = rng.choice([64, 128, 256, 512], size=256)
+    params = [th.params.default_params(xlen=int(e), ylen=int(e), lsx=0.1, lsy=0.1, time_step=0.02,
+                                       kappa=float(rng.uniform(0.5, 2)), mpi=float(rng.uniform(0.5, 2)),
+                                       unit_magnetization=True) for e in edges]
+    b = BatchSolver(th, params, "fp32", device=dev)
+    for i, p in enumerate(params):
+        b.load(i, hedgehog(p.resolved(), charge=int(rng.integers(1, 5)), R=float(rng.uniform(1, 3)), seed=i,
+                           device=dev))
+    b.step(3, 1e300)
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter()
+    E, _ = b.step(steps)
+    torch.cuda.synchronize(dev)
+    dt = time.perf_counter() - t
+    sites = int(sum(int(e) * int(e) for e in edges))
+    return {"lattices": 256, "sites": sites, "steps": steps, "value": sites * steps / dt / 1e6, "unit": UNIT,
+            "ms_per_step": dt / steps * 1e3, "tma": b.tma_enabled, "finite": bool(np.isfinite(E).all()),
+            "note": "ss_batch_step: one launch per RK stage over all 256 lattices, wall clock incl. host sync"}
+
+
 def compare_fp64_and_plain(args, dev, F0):
     """Relaxed-state accuracy (320^2), and the plain-FP64 form's speed on this lattice."""
     import torch
     from soliton_solver_b200.core.simulation import Simulation
     th, p = chiral_params()
-    out = {"accuracy": relaxed_accuracy(dev)}
+    out = {"accuracy": relaxed_accuracy(dev), "batched_sweep": batched_sweep(dev)}
     sim = Simulation(p, th, precision="plain_fp64", device=dev)
     sim.load_field(F0)
     sim.relax(1, 1e300)

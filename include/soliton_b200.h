@@ -73,6 +73,7 @@ extern "C" {
 #define SS_COUPLING_COUP_MU 5 /* chiral magnet coup_mu (p_f[8]) */
 
 typedef struct ss_handle ss_handle;
+typedef struct ss_batch ss_batch;
 
 int ss_abi_version(void);
 const char *ss_status_string(int status);
@@ -179,6 +180,25 @@ int ss_rk4_stage(ss_handle *h, void *k_out, const void *velocity, const void *l_
 int ss_rk4_finalize(ss_handle *h, void *velocity, void *field, const void *k1, const void *k2,
                     const void *k3, const void *k4, const void *l1, const void *l2, const void *l3,
                     const void *l4);
+
+/* ---- batches: many independent lattices of one theory ----------------------
+ * The lattices may differ in size, couplings and state; each keeps its own arrest
+ * flag and energy.  One launch per RK stage covers every lattice's tiles.  No
+ * reference counterpart (the reference runs one lattice per Simulation); each
+ * lattice's step is exactly ss_step's.
+ * p_i / p_f hold n_lattices packed arrays of n_i / n_f entries back to back. */
+int ss_batch_create(int theory, int n_lattices, const int32_t *p_i, int n_i, const double *p_f, int n_f,
+                    int precision, ss_batch **out);
+int ss_batch_destroy(ss_batch *b);
+int ss_batch_workspace_bytes(const ss_batch *b, size_t *bytes);
+/* fields[i] / velocities[i]: device buffers of lattice i (caller-owned). */
+int ss_batch_bind(ss_batch *b, void *const *fields, void *const *velocities, void *workspace,
+                  size_t workspace_bytes, void *stream);
+/* n_steps steps of every lattice.  prev_energy (host, n_lattices, nullable: continue
+ * from the device state) seeds each first arrest test; energy_traj / err_traj (host,
+ * nullable) receive lattice-major [i * n_steps + s] trajectories. */
+int ss_batch_step(ss_batch *b, int n_steps, const double *prev_energy, double *energy_traj, double *err_traj);
+int ss_batch_tma_enabled(const ss_batch *b);
 
 #ifdef __cplusplus
 }

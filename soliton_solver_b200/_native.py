@@ -91,6 +91,12 @@ _SIG = {
     "ss_coupling_grad": ([_P, _P, _I, ctypes.POINTER(_D)], _I),
     "ss_energy_noalloc": ([_I, _P, _I, _P, _I, _I, _P, ctypes.POINTER(_D), _P], _I),
     "ss_rk4_stage": ([_P, _P, _P, _P, _P, _P, _P, _D], _I),
+    "ss_batch_create": ([_I, _I, _P, _I, _P, _I, _I, ctypes.POINTER(_P)], _I),
+    "ss_batch_destroy": ([_P], _I),
+    "ss_batch_workspace_bytes": ([_P, ctypes.POINTER(ctypes.c_size_t)], _I),
+    "ss_batch_bind": ([_P, _P, _P, _P, ctypes.c_size_t, _P], _I),
+    "ss_batch_step": ([_P, _I, _P, _P, _P], _I),
+    "ss_batch_tma_enabled": ([_P], _I),
     "ss_rk4_finalize": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
 }
 EXPORTS = tuple(_SIG)

@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "flow.cuh"
 #include "plain.cuh"
+#include "batch.cuh"
 #include "theories.cuh"
 
 using namespace ssb;
@@ -1124,3 +1125,251 @@ extern "C" int ss_energy_noalloc(int theory, const int32_t* p_i, int n_i, const 
   if (s.status) return fail(SS_ERR_NONFINITE, "the energy reduction produced a non-finite value");
   return SS_OK;
 }
+
+
+// ===========================================================================
+// Batched lattices: many independent relaxations of one theory per launch
+// ===========================================================================
+struct ss_batch {
+  int theory = 0, precision = 0, n = 0, nf = 0;
+  size_t elem = 4;
+  std::vector<ss_handle> inst;   // decoded parameters per lattice (host only)
+  std::vector<int> tiles;        // tiles per lattice
+  int total_tiles = 0;
+  bool tma = false;
+  cudaStream_t stream = nullptr;
+  char* ws = nullptr;
+  BatchInst* d_insts = nullptr;
+  int* d_tile_inst = nullptr;
+  double* d_prev = nullptr;
+  std::vector<BatchInst> h_insts;
+  std::vector<void*> fields, vels;
+  long long wait_cycles = WAIT_CYCLES;
+};
+
+namespace {
+
+size_t batch_layout(ss_batch* b, char* base) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> char* {
+    char* p = base ? base + off : nullptr;
+    off = align_up(off + bytes);
+    return p;
+  };
+  b->d_insts = (BatchInst*)take(sizeof(BatchInst) * b->n);
+  b->d_tile_inst = (int*)take(sizeof(int) * b->total_tiles);
+  b->d_prev = (double*)take(sizeof(double) * b->n);
+  b->h_insts.assign(b->n, BatchInst{});
+  for (int i = 0; i < b->n; ++i) {
+    BatchInst& I = b->h_insts[i];
+    const size_t fb = b->elem * (size_t)b->nf * (size_t)b->inst[i].G.N;
+    I.st = (StepState*)take(sizeof(StepState));
+    I.partial = (double*)take(sizeof(double) * b->tiles[i]);
+    I.E_traj = (double*)take(sizeof(double) * TRAJ_CAP);
+    I.err_traj = (double*)take(sizeof(double) * TRAJ_CAP);
+    for (int k = 2; k < 7; ++k) I.buf[k] = take(fb);
+  }
+  return off;
+}
+
+template <class TH, typename R>
+struct Batched {
+  static constexpr size_t BUF = tile_buf_bytes<R, TH::NF, TX, TY>();
+  static inline unsigned long long smem_done[2][6] = {};
+
+  template <bool TMA_, int MODE>
+  static int launch_mode(const ss_batch* b, const BatchStep& B) {
+    auto k = batch_flow_kernel<TH, R, TX, TY, NT, TMA_, MODE>;
+    const size_t smem = TMA_ ? flow_buffers(MODE) * BUF : BUF;
+    set_smem(k, smem, smem_done[TMA_ ? 1 : 0][MODE]);
+    k<<<b->total_tiles, NT, smem, b->stream>>>(b->d_insts, b->d_tile_inst, B);
+    CK(cudaGetLastError());
+    return SS_OK;
+  }
+  template <int MODE>
+  static int launch(const ss_batch* b, const BatchStep& B) {
+    return b->tma ? launch_mode<true, MODE>(b, B) : launch_mode<false, MODE>(b, B);
+  }
+
+  static int step(ss_batch* b, int n, bool use_prev) {
+    if (n <= 0) return SS_OK;
+    BatchStep B;
+    memset(&B, 0, sizeof(B));
+    B.wait_cycles = b->wait_cycles;
+    int parity = 0, rc;
+    for (int s = 0; s < n; ++s) {
+      B.parity = parity;
+      B.with_energy = s > 0;
+      B.arrest_update = s > 0;
+      B.init_state = s == 0;
+      B.prev_energy = (s == 0 && use_prev) ? b->d_prev : nullptr;
+      B.E_idx = s - 1;
+      B.err_idx = -1;
+      if ((rc = launch<M_S1>(b, B))) return rc;
+      B.with_energy = B.arrest_update = B.init_state = 0;
+      B.prev_energy = nullptr;
+      B.E_idx = -1;
+      if ((rc = launch<M_S2>(b, B))) return rc;
+      if ((rc = launch<M_S3>(b, B))) return rc;
+      B.err_idx = s;
+      if ((rc = launch<M_S4>(b, B))) return rc;
+      B.err_idx = -1;
+      parity ^= 1;
+    }
+    B.parity = parity;
+    B.with_energy = B.arrest_update = 1;
+    B.E_idx = n - 1;
+    if ((rc = launch<M_ENERGY>(b, B))) return rc;
+    batch_finish_kernel<R, TH::NF><<<dim3(64, b->n), 256, 0, b->stream>>>(b->d_insts, parity);
+    CK(cudaGetLastError());
+    return SS_OK;
+  }
+};
+
+template <class Fn>
+int batch_dispatch(const ss_batch* b, Fn&& fn) {
+  switch (b->theory) {
+    case SS_THEORY_CHIRAL_MAGNET: return fn((ChiralMagnet*)nullptr);
+    case SS_THEORY_BABY_SKYRME: return fn((BabySkyrme*)nullptr);
+    case SS_THEORY_GINZBURG_LANDAU: return fn((GinzburgLandau*)nullptr);
+    case SS_THEORY_ANISOTROPIC: return fn((Anisotropic*)nullptr);
+  }
+  return fail(SS_ERR_ARG, "bad theory");
+}
+
+}  // namespace
+
+extern "C" {
+
+int ss_batch_create(int theory, int n_lattices, const int32_t* p_i, int n_i, const double* p_f, int n_f,
+                    int precision, ss_batch** out) {
+  if (!out) return fail(SS_ERR_ARG, "out must not be NULL");
+  *out = nullptr;
+  if (n_lattices < 1) return fail(SS_ERR_ARG, "n_lattices must be >= 1");
+  if (precision != SS_FP32 && precision != SS_FP64) return fail(SS_ERR_ARG, "batches support SS_FP32 and SS_FP64");
+  ss_batch* b = new ss_batch();
+  b->theory = theory;
+  b->precision = precision;
+  b->n = n_lattices;
+  b->elem = precision == SS_FP32 ? 4 : 8;
+  b->inst.resize(n_lattices);
+  long long total = 0;
+  for (int i = 0; i < n_lattices; ++i) {
+    ss_handle& h = b->inst[i];
+    int rc = decode(&h, theory, p_i + (size_t)i * n_i, n_i, p_f + (size_t)i * n_f, n_f);
+    if (rc) {
+      char msg[sizeof(g_err)];
+      snprintf(msg, sizeof(msg), "%s", g_err);
+      delete b;
+      return fail(rc, "lattice %d: %s", i, msg);
+    }
+    const long long t = (long long)((h.G.X + TX - 1) / TX) * ((h.G.Y + TY - 1) / TY);
+    b->tiles.push_back((int)t);
+    total += t;
+  }
+  if (total > 0x7fffffffLL) {
+    delete b;
+    return fail(SS_ERR_ARG, "batch too large");
+  }
+  b->total_tiles = (int)total;
+  b->nf = b->inst[0].nf;
+  *out = b;
+  return SS_OK;
+}
+
+int ss_batch_destroy(ss_batch* b) {
+  delete b;
+  return SS_OK;
+}
+
+int ss_batch_workspace_bytes(const ss_batch* b, size_t* bytes) {
+  if (!b || !bytes) return fail(SS_ERR_ARG, "NULL argument");
+  ss_batch tmp = *b;
+  *bytes = batch_layout(&tmp, nullptr);
+  return SS_OK;
+}
+
+int ss_batch_bind(ss_batch* b, void* const* fields, void* const* velocities, void* workspace, size_t workspace_bytes,
+                  void* stream) {
+  if (!b || !fields || !velocities || !workspace) return fail(SS_ERR_ARG, "NULL argument");
+  if (((uintptr_t)workspace) % ALIGN) return fail(SS_ERR_WORKSPACE, "workspace must be %zu-byte aligned", ALIGN);
+  size_t need = 0;
+  ss_batch_workspace_bytes(b, &need);
+  if (workspace_bytes < need) return fail(SS_ERR_WORKSPACE, "workspace has %zu bytes, needs %zu", workspace_bytes, need);
+  b->ws = (char*)workspace;
+  b->stream = (cudaStream_t)stream;
+  batch_layout(b, b->ws);
+  b->fields.assign(fields, fields + b->n);
+  b->vels.assign(velocities, velocities + b->n);
+  bool tma = true;
+  int tile0 = 0;
+  std::vector<int> tile_inst(b->total_tiles);
+  for (int i = 0; i < b->n; ++i) {
+    BatchInst& I = b->h_insts[i];
+    if (!fields[i] || !velocities[i]) return fail(SS_ERR_ARG, "lattice %d: NULL field or velocity", i);
+    I.G = b->inst[i].G;
+    I.P = b->inst[i].P;
+    I.buf[0] = fields[i];
+    I.buf[1] = velocities[i];
+    I.tile0 = tile0;
+    I.ntiles = b->tiles[i];
+    for (int t = 0; t < I.ntiles; ++t) tile_inst[tile0 + t] = i;
+    tile0 += I.ntiles;
+    for (int k = 0; k < 6 && tma; ++k) tma = encode_tile_map(&I.tm[k], I.buf[k], b->elem, I.G.X, I.G.Y, b->nf);
+  }
+  b->tma = tma;
+  StepState init;
+  memset(&init, 0, sizeof(init));
+  init.E_last = NAN;
+  for (int i = 0; i < b->n; ++i)
+    CK(cudaMemcpyAsync(b->h_insts[i].st, &init, sizeof(init), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_insts, b->h_insts.data(), sizeof(BatchInst) * b->n, cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_tile_inst, tile_inst.data(), sizeof(int) * b->total_tiles, cudaMemcpyHostToDevice,
+                     b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return SS_OK;
+}
+
+int ss_batch_step(ss_batch* b, int n_steps, const double* prev_energy, double* energy_traj, double* err_traj) {
+  if (!b || !b->ws) return fail(SS_ERR_STATE, "batch not bound");
+  if (n_steps < 0) return fail(SS_ERR_ARG, "n_steps must be >= 0");
+  if (prev_energy)
+    CK(cudaMemcpyAsync(b->d_prev, prev_energy, sizeof(double) * b->n, cudaMemcpyHostToDevice, b->stream));
+  bool use_prev = prev_energy != nullptr;
+  for (int done = 0; done < n_steps; done += TRAJ_CAP) {
+    const int k = std::min(TRAJ_CAP, n_steps - done);
+    int rc = batch_dispatch(b, [&](auto* tag) -> int {
+      using TH = std::remove_pointer_t<decltype(tag)>;
+      if (b->precision == SS_FP32) return Batched<TH, float>::step(b, k, use_prev);
+      return Batched<TH, double>::step(b, k, use_prev);
+    });
+    if (rc) return rc;
+    use_prev = false;
+    for (int i = 0; i < b->n; ++i) {
+      if (energy_traj)
+        CK(cudaMemcpyAsync(energy_traj + (size_t)i * n_steps + done, b->h_insts[i].E_traj, k * sizeof(double),
+                           cudaMemcpyDeviceToHost, b->stream));
+      if (err_traj)
+        CK(cudaMemcpyAsync(err_traj + (size_t)i * n_steps + done, b->h_insts[i].err_traj, k * sizeof(double),
+                           cudaMemcpyDeviceToHost, b->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(b->stream));
+  int worst = 0;
+  for (int i = 0; i < b->n; ++i) {
+    StepState st;
+    CK(cudaMemcpy(&st, b->h_insts[i].st, sizeof(st), cudaMemcpyDeviceToHost));
+    if (st.status) {
+      worst = st.status;
+      const int zero = 0;
+      CK(cudaMemcpy(&b->h_insts[i].st->status, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    }
+  }
+  if (worst == SS_ERR_TIMEOUT) return fail(SS_ERR_TIMEOUT, "a device-side wait timed out; re-bind the batch");
+  if (worst) return fail(SS_ERR_NONFINITE, "a lattice's energy became non-finite");
+  return SS_OK;
+}
+
+int ss_batch_tma_enabled(const ss_batch* b) { return b && b->tma ? 1 : 0; }
+
+}  // extern "C"

@@ -1,0 +1,101 @@
+// batch.cuh -- many independent lattices of one theory advanced together.
+//
+// One launch per RK stage covers the tiles of every lattice: block b works on tile
+// b - tile0[i] of lattice i = tile_inst[b].  Each lattice keeps its own parameters,
+// buffers, reduction partials and device step state (energy, arrest flag, err), so
+// sizes, couplings and arrest histories are independent; the per-lattice last block
+// (ticket counted per lattice) finalises that lattice's reductions.
+#pragma once
+
+#include "flow.cuh"
+
+namespace ssb {
+
+struct BatchInst {
+  CUtensorMap tm[6];  // halo-box TMA maps: field, velocity, phi_alt, vel_alt, l1, l2
+  Grid G;
+  Phys P;
+  void* buf[7];       // field, velocity, phi_alt, vel_alt, l1, l2, l3
+  StepState* st;
+  double* partial;    // one slot per tile of this lattice
+  double* E_traj;     // per-lattice trajectory rows
+  double* err_traj;
+  int tile0, ntiles;
+};
+
+struct BatchStep {
+  int parity;         // 0: the caller's buffers hold the current field; 1: the alternates do
+  int with_energy, arrest_update, init_state;
+  int E_idx, err_idx;
+  const double* prev_energy;  // device, one per lattice (NaN keeps E_last); read with init_state
+  long long wait_cycles;
+};
+
+template <class TH, typename R, int TX, int TY, int NT, bool TMA, int MODE>
+__global__ void __launch_bounds__(NT)
+    batch_flow_kernel(const BatchInst* __restrict__ insts, const int* __restrict__ tile_inst,
+                      const __grid_constant__ BatchStep B) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ StageShared<NT> S;
+  __shared__ FlowArgs<R> A;
+  const int inst = tile_inst[blockIdx.x];
+  const BatchInst& I = insts[inst];
+  {  // the lattice's parameters into shared memory (word copy)
+    const int* src = reinterpret_cast<const int*>(&I.G);
+    int* dst = reinterpret_cast<int*>(&A.G);
+    for (int i = threadIdx.x; i < (int)(sizeof(Grid) / 4); i += NT) dst[i] = src[i];
+    src = reinterpret_cast<const int*>(&I.P);
+    dst = reinterpret_cast<int*>(&A.P);
+    for (int i = threadIdx.x; i < (int)(sizeof(Phys) / 4); i += NT) dst[i] = src[i];
+  }
+  const int cur = B.parity;
+  if (threadIdx.x == 0) {
+    A.phi = (const R*)I.buf[cur ? 2 : 0];
+    A.vel = (const R*)I.buf[cur ? 3 : 1];
+    A.la = (const R*)I.buf[4];
+    A.lb = (const R*)I.buf[5];
+    A.lc = (const R*)I.buf[6];
+    A.out_l = MODE == M_S1 ? (R*)I.buf[4] : MODE == M_S2 ? (R*)I.buf[5] : MODE == M_S3 ? (R*)I.buf[6] : nullptr;
+    A.out_eg = nullptr;
+    A.phi_out = (R*)I.buf[cur ? 0 : 2];
+    A.vel_out = (R*)I.buf[cur ? 1 : 3];
+    A.partial = I.partial;
+    A.st = I.st;
+    A.E_traj = I.E_traj;
+    A.err_traj = I.err_traj;
+    A.E_idx = B.E_idx;
+    A.err_idx = B.err_idx;
+    A.mode = MODE;
+    A.with_energy = B.with_energy;
+    A.arrest_update = B.arrest_update;
+    A.init_state = B.init_state;
+    A.prev_energy = B.prev_energy ? B.prev_energy[inst] : NAN;
+    A.grad_raw = 0;
+    A.wait_cycles = B.wait_cycles;
+    A.tx_extra = 0;
+  }
+  __syncthreads();
+  flow_tile<TH, R, TX, TY, NT, TMA, MODE>(A, &I.tm[cur ? 2 : 0], &I.tm[cur ? 3 : 1], &I.tm[MODE == M_S3 ? 4 : 5],
+                                          blockIdx.x - I.tile0, I.ntiles, smem_raw, S);
+}
+
+// Copy each lattice's result back into the caller's buffers when the alternates hold
+// it, and apply a pending arrest (V = 0).  grid.y = lattice.
+template <typename R, int NF>
+__global__ void batch_finish_kernel(const BatchInst* __restrict__ insts, int parity) {
+  const BatchInst& I = insts[blockIdx.y];
+  const bool arrest = I.st->arrest != 0;
+  const bool copy = parity != 0;
+  if (!copy && !arrest) return;
+  R* dp = (R*)I.buf[0];
+  R* dv = (R*)I.buf[1];
+  const R* sp = (const R*)I.buf[2];
+  const R* sv = (const R*)I.buf[3];
+  const long long n = (long long)NF * I.G.N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if (copy) dp[i] = sp[i];
+    dv[i] = arrest ? (R)0 : (copy ? sv[i] : dv[i]);
+  }
+}
+
+}  // namespace ssb

@@ -450,30 +450,43 @@ __device__ __forceinline__ double energy_tile(const FlowArgs<R>& A, const E* T, 
   return e_acc;
 }
 
+// Shared scratch of the one-tile-per-CTA stage kernels besides the staged tile.
+template <int NT>
+struct StageShared {
+  double red[NT / 32];
+  double sh_s[NT], sh_c[NT];
+  uint64_t bar;
+  int am_last;
+};
+
+// Stage, compute and reduce tile `tile` of a lattice of `nblk` tiles (one CTA per
+// tile).  tm_phi / tm_vel / tm_l are TMA maps in parameter or global memory.
 template <class TH, typename R, int TX, int TY, int NT, bool TMA, int MODE>
-__global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowArgs<R> A) {
+__device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMap* tm_phi, const CUtensorMap* tm_vel,
+                                          const CUtensorMap* tm_l, int tile, int nblk, unsigned char* smem_raw,
+                                          StageShared<NT>& S) {
   using TS = TileShape<TX, TY, NT>;
   constexpr int NF = TH::NF;
   constexpr int BUF = NF * TS::PLANE;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
   R* B0 = reinterpret_cast<R*>(smem_raw);
   R* B1 = B0 + BUF;
   R* B2 = B1 + BUF;
-  __shared__ double red[NT / 32];
-  __shared__ double sh_s[NT], sh_c[NT];
-  __shared__ int am_last;
-  __shared__ __align__(8) uint64_t bar;
+  double* red = S.red;
+  double* sh_s = S.sh_s;
+  double* sh_c = S.sh_c;
+  uint64_t& bar = S.bar;
+  int& am_last = S.am_last;
 
   const Grid& G = A.G;
   constexpr int mode = MODE;
   const int tiles_y = (G.Y + TY - 1) / TY;
-  const int x0 = (blockIdx.x / tiles_y) * TX;
-  const int y0 = (blockIdx.x % tiles_y) * TY;
+  const int x0 = (tile / tiles_y) * TX;
+  const int y0 = (tile % tiles_y) * TY;
   StepState* st = A.st;
   const bool arrest = (mode == M_S2 || mode == M_S3 || mode == M_S4) && (st->arrest != 0);
   const bool do_energy = (MODE == M_S1 || MODE == M_ENERGY) && A.with_energy != 0;
 
-  if (A.init_state && blockIdx.x == 0 && threadIdx.x == 0) {
+  if (A.init_state && tile == 0 && threadIdx.x == 0) {
     st->arrest = 0;
     if (!isnan(A.prev_energy)) st->E_last = A.prev_energy;
   }
@@ -488,9 +501,9 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
     if (threadIdx.x == 0) {
       const uint32_t bytes = (uint32_t)(sizeof(R) * BUF) * (1u + (need_v ? 1u : 0u) + (need_l ? 1u : 0u));
       mbar_expect_tx(&bar, bytes + A.tx_extra);
-      tma_load_3d(B0, &A.tm_phi, y0 - TS::YOFF, x0 - 2, 0, &bar);
-      if (need_v) tma_load_3d(B1, &A.tm_vel, y0 - TS::YOFF, x0 - 2, 0, &bar);
-      if (need_l) tma_load_3d(B2, &A.tm_l, y0 - TS::YOFF, x0 - 2, 0, &bar);
+      tma_load_3d(B0, tm_phi, y0 - TS::YOFF, x0 - 2, 0, &bar);
+      if (need_v) tma_load_3d(B1, tm_vel, y0 - TS::YOFF, x0 - 2, 0, &bar);
+      if (need_l) tma_load_3d(B2, tm_l, y0 - TS::YOFF, x0 - 2, 0, &bar);
     }
     const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0, A.wait_cycles));
     if (!ok) {
@@ -565,7 +578,7 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
   if (!need_ticket) return;
   if (do_energy) {
     const double bs = block_sum_fixed<NT>(e_acc, red);
-    if (threadIdx.x == 0) A.partial[blockIdx.x] = bs;
+    if (threadIdx.x == 0) A.partial[tile] = bs;
   }
   if (mode == M_S4) {
     const double bm = block_max<NT>(err_max, red);
@@ -574,13 +587,13 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned t = atomicAdd(&st->ticket, 1u);
-    am_last = (t == gridDim.x - 1);
+    am_last = (t == (unsigned)nblk - 1u);
   }
   __syncthreads();
   if (!am_last) return;
   __threadfence();
   if (do_energy) {
-    const double E = fixed_order_sum<NT>(A.partial, gridDim.x, sh_s, sh_c);
+    const double E = fixed_order_sum<NT>(A.partial, nblk, sh_s, sh_c);
     if (threadIdx.x == 0) {
       st->scalar = E;
       if (!isfinite(E)) st->status = 3;
@@ -598,6 +611,13 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
     }
     st->ticket = 0u;
   }
+}
+
+template <class TH, typename R, int TX, int TY, int NT, bool TMA, int MODE>
+__global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowArgs<R> A) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ StageShared<NT> S;
+  flow_tile<TH, R, TX, TY, NT, TMA, MODE>(A, &A.tm_phi, &A.tm_vel, &A.tm_l, blockIdx.x, gridDim.x, smem_raw, S);
 }
 
 // ---------------------------------------------------------------------------
