@@ -200,6 +200,19 @@ int ss_batch_bind(ss_batch *b, void *const *fields, void *const *velocities, voi
 int ss_batch_step(ss_batch *b, int n_steps, const double *prev_energy, double *energy_traj, double *err_traj);
 int ss_batch_tma_enabled(const ss_batch *b);
 
+/* ---- CUDA graphs ---------------------------------------------------------------
+ * ss_graph_create captures n_steps of ss_step_async(h, n_steps, NaN, ...) — every
+ * stage launch, the trailing energy pass and the copy-back — into a CUDA graph on a
+ * private stream; ss_graph_launch replays it on the bound stream (each replay
+ * continues from the device state).  The batch versions capture n_steps (at most
+ * 1024) of every lattice; ss_batch_trajectory copies the last replay's per-lattice
+ * trajectories to the host.  No reference counterpart. */
+int ss_graph_create(ss_handle *h, int n_steps, double *energy_traj_dev, double *err_traj_dev);
+int ss_graph_launch(ss_handle *h);
+int ss_batch_graph_create(ss_batch *b, int n_steps);
+int ss_batch_graph_launch(ss_batch *b);
+int ss_batch_trajectory(ss_batch *b, int n_steps, double *energy_traj, double *err_traj);
+
 #ifdef __cplusplus
 }
 #endif

@@ -97,6 +97,11 @@ _SIG = {
     "ss_batch_bind": ([_P, _P, _P, _P, ctypes.c_size_t, _P], _I),
     "ss_batch_step": ([_P, _I, _P, _P, _P], _I),
     "ss_batch_tma_enabled": ([_P], _I),
+    "ss_graph_create": ([_P, _I, _P, _P], _I),
+    "ss_graph_launch": ([_P], _I),
+    "ss_batch_graph_create": ([_P, _I], _I),
+    "ss_batch_graph_launch": ([_P], _I),
+    "ss_batch_trajectory": ([_P, _I, _P, _P], _I),
     "ss_rk4_finalize": ([_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
 }
 EXPORTS = tuple(_SIG)

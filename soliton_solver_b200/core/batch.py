@@ -71,6 +71,24 @@ class BatchSolver:
                                               E.ctypes.data, err.ctypes.data))
         return E, err
 
+    def capture(self, n_steps: int):
+        """Capture n_steps (<= 1024) of every lattice into a CUDA graph."""
+        self._graph_steps = int(n_steps)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_batch_graph_create(self._h, int(n_steps)))
+
+    def replay(self):
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_batch_graph_launch(self._h))
+
+    def trajectory(self):
+        """(energy, err) of the last graph replay, shape (n_lattices, captured steps)."""
+        n = self._graph_steps
+        E = np.empty((self.n, n))
+        err = np.empty((self.n, n))
+        nat.check(self._lib.ss_batch_trajectory(self._h, n, E.ctypes.data, err.ctypes.data))
+        return E, err
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None:

@@ -115,6 +115,22 @@ class Solver:
             nat.check(self._lib.ss_step_async(self._h, int(n_steps), float(prev_energy), _ptr(energy_traj),
                                               _ptr(err_traj)))
 
+    def capture(self, n_steps: int, energy_traj=None, err_traj=None):
+        """Capture n_steps of step_async into a CUDA graph (replay with replay())."""
+        for t in (energy_traj, err_traj):
+            if t is not None:
+                self._check(t, torch.float64)
+                if t.numel() < n_steps:
+                    raise ValueError("trajectory buffer shorter than n_steps")
+        self._graph_bufs = (energy_traj, err_traj)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_graph_create(self._h, int(n_steps), _ptr(energy_traj), _ptr(err_traj)))
+
+    def replay(self):
+        """Launch the captured graph on the bound stream (no host synchronisation)."""
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_graph_launch(self._h))
+
     @property
     def tma_enabled(self) -> bool:
         """True when the bound buffers are staged with TMA tensor maps."""

@@ -118,6 +118,10 @@ struct ss_handle {
   float tune_ms[6][2] = {};
   long long wait_cycles = WAIT_CYCLES;
   mutable int inject_timeout = 0;  // test hook, consumed by the next flow launch
+  cudaGraphExec_t graph = nullptr;  // captured n-step relaxation (ss_graph_create)
+  ~ss_handle() {
+    if (graph) cudaGraphExecDestroy(graph);
+  }
 };
 
 namespace {
@@ -808,6 +812,7 @@ int ss_destroy(ss_handle* h) {
 int ss_workspace_bytes(const ss_handle* h, size_t* bytes) {
   if (!h || !bytes) return fail(SS_ERR_ARG, "NULL argument");
   ss_handle tmp = *h;
+  tmp.graph = nullptr;  // the copy must not own the original's graph
   *bytes = layout(&tmp, nullptr);
   return SS_OK;
 }
@@ -1145,6 +1150,10 @@ struct ss_batch {
   std::vector<BatchInst> h_insts;
   std::vector<void*> fields, vels;
   long long wait_cycles = WAIT_CYCLES;
+  cudaGraphExec_t graph = nullptr;
+  ~ss_batch() {
+    if (graph) cudaGraphExecDestroy(graph);
+  }
 };
 
 namespace {
@@ -1285,6 +1294,7 @@ int ss_batch_destroy(ss_batch* b) {
 int ss_batch_workspace_bytes(const ss_batch* b, size_t* bytes) {
   if (!b || !bytes) return fail(SS_ERR_ARG, "NULL argument");
   ss_batch tmp = *b;
+  tmp.graph = nullptr;  // the copy must not own the original's graph
   *bytes = batch_layout(&tmp, nullptr);
   return SS_OK;
 }
@@ -1371,5 +1381,94 @@ int ss_batch_step(ss_batch* b, int n_steps, const double* prev_energy, double* e
 }
 
 int ss_batch_tma_enabled(const ss_batch* b) { return b && b->tma ? 1 : 0; }
+
+}  // extern "C"
+
+
+// ===========================================================================
+// CUDA graphs of whole relaxations
+// ===========================================================================
+namespace {
+
+// Capture `issue` (which launches on *stream_slot) on a private stream into a graph.
+template <class Issue>
+int capture_graph(cudaStream_t* stream_slot, cudaGraphExec_t* out, Issue&& issue) {
+  cudaStream_t cs;
+  CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaStream_t saved = *stream_slot;
+  *stream_slot = cs;
+  cudaGraph_t g = nullptr;
+  int rc = SS_OK;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+  if (e == cudaSuccess) {
+    rc = issue();
+    cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+    if (rc == SS_OK && e2 != cudaSuccess) rc = fail(SS_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e2));
+  } else {
+    rc = fail(SS_ERR_CUDA, "cudaStreamBeginCapture: %s", cudaGetErrorString(e));
+  }
+  *stream_slot = saved;
+  if (rc == SS_OK) {
+    if (*out) cudaGraphExecDestroy(*out);
+    *out = nullptr;
+    e = cudaGraphInstantiate(out, g, 0);
+    if (e != cudaSuccess) rc = fail(SS_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cs);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ss_graph_create(ss_handle* h, int n_steps, double* energy_traj_dev, double* err_traj_dev) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (n_steps < 1) return fail(SS_ERR_ARG, "n_steps must be >= 1");
+  if (h->precision == SS_PLAIN_FP64) return fail(SS_ERR_ARG, "the plain FP64 form arrests on the host");
+  return capture_graph(&h->stream, &h->graph,
+                       [&]() { return ss_step_async(h, n_steps, NAN, energy_traj_dev, err_traj_dev); });
+}
+
+int ss_graph_launch(ss_handle* h) {
+  if (!h || !h->graph) return fail(SS_ERR_STATE, "no graph captured: call ss_graph_create");
+  CK(cudaGraphLaunch(h->graph, h->stream));
+  return SS_OK;
+}
+
+int ss_batch_graph_create(ss_batch* b, int n_steps) {
+  if (!b || !b->ws) return fail(SS_ERR_STATE, "batch not bound");
+  if (n_steps < 1 || n_steps > TRAJ_CAP) return fail(SS_ERR_ARG, "n_steps must be in 1..%d", TRAJ_CAP);
+  return capture_graph(&b->stream, &b->graph, [&]() {
+    return batch_dispatch(b, [&](auto* tag) -> int {
+      using TH = std::remove_pointer_t<decltype(tag)>;
+      if (b->precision == SS_FP32) return Batched<TH, float>::step(b, n_steps, false);
+      return Batched<TH, double>::step(b, n_steps, false);
+    });
+  });
+}
+
+int ss_batch_graph_launch(ss_batch* b) {
+  if (!b || !b->graph) return fail(SS_ERR_STATE, "no graph captured: call ss_batch_graph_create");
+  CK(cudaGraphLaunch(b->graph, b->stream));
+  return SS_OK;
+}
+
+int ss_batch_trajectory(ss_batch* b, int n_steps, double* energy_traj, double* err_traj) {
+  if (!b || !b->ws) return fail(SS_ERR_STATE, "batch not bound");
+  if (n_steps < 0 || n_steps > TRAJ_CAP) return fail(SS_ERR_ARG, "n_steps must be in 0..%d", TRAJ_CAP);
+  for (int i = 0; i < b->n; ++i) {
+    if (energy_traj)
+      CK(cudaMemcpyAsync(energy_traj + (size_t)i * n_steps, b->h_insts[i].E_traj, n_steps * sizeof(double),
+                         cudaMemcpyDeviceToHost, b->stream));
+    if (err_traj)
+      CK(cudaMemcpyAsync(err_traj + (size_t)i * n_steps, b->h_insts[i].err_traj, n_steps * sizeof(double),
+                         cudaMemcpyDeviceToHost, b->stream));
+  }
+  CK(cudaStreamSynchronize(b->stream));
+  return SS_OK;
+}
 
 }  // extern "C"
