@@ -142,6 +142,14 @@ int ss_energy_density(ss_handle *h, const void *field, double *density);
 /* Total energy, fixed-order compensated FP64 sum.  Replaces observables.compute_energy
  * (e.g. theories/chiral_magnet/observables.py:15-57). */
 int ss_energy(ss_handle *h, const void *field, double *out);
+/* Total FP64 energy (as ss_energy) of the field with each site's unit-vector
+ * components divided by their FP64 norm: the normalisation of the reference's RK4
+ * finalize (core/integrator.py:151-189) applied in FP64 before
+ * observables.compute_energy.  For an FP32 field it removes the bias of m3 rounding to 1
+ * where |m_perp| < 2.4e-4 (|m|^2 - 1 = |m_perp|^2 there); for theories without a
+ * unit-vector constraint it equals the FP64 energy of the field.  Uses the l-buffer
+ * part of the bound workspace.  No reference counterpart (new observable). */
+int ss_energy_projected(ss_handle *h, const void *field, double *out);
 /* Charge densities / totals.  Replace compute_skyrmion_number_kernel,
  * compute_magnetic_charge_kernel, compute_vortex_number_kernel and the matching
  * observables.compute_* (e.g. theories/chiral_magnet/kernels.py:294-395,

@@ -86,6 +86,7 @@ _SIG = {
     "ss_energy_gradient": ([_P, _P, _P], _I),
     "ss_energy_density": ([_P, _P, _P], _I),
     "ss_energy": ([_P, _P, ctypes.POINTER(_D)], _I),
+    "ss_energy_projected": ([_P, _P, ctypes.POINTER(_D)], _I),
     "ss_charge_density": ([_P, _P, _I, _P], _I),
     "ss_charge": ([_P, _P, _I, ctypes.POINTER(_D)], _I),
     "ss_coupling_grad": ([_P, _P, _I, ctypes.POINTER(_D)], _I),

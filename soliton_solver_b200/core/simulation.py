@@ -116,6 +116,16 @@ class Simulation:
             obs["magnetic_charge"] = self.solver.charge(self.Field, "magnetic")
         return obs
 
+    def projected_energy(self) -> float:
+        """FP64 energy of sim.Field with every site's magnetisation divided by its FP64
+        norm.  For an FP32 relaxation this is the energy of the relaxed state on the
+        constraint manifold: the stored FP32 m3 rounds to 1 wherever |m_perp| < 2.4e-4,
+        which drops the |m_perp|^2 / 2 that the Zeeman and anisotropy terms should see
+        there and biases the plain energy of a large vacuum downwards.  Equal to
+        observables()["energy"] to FP64 rounding for FP64 fields and for theories
+        without a unit-vector constraint."""
+        return self.solver.energy_projected(self.Field)
+
     def compute_energy_density(self):
         self.solver.energy_density(self.Field, self.en)
         torch.cuda.synchronize(self.device)

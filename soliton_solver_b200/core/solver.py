@@ -182,6 +182,15 @@ class Solver:
             nat.check(self._lib.ss_energy(self._h, _ptr(field), ctypes.byref(out)))
         return out.value
 
+    def energy_projected(self, field) -> float:
+        """FP64 energy of `field` with each site's unit vector renormalised in FP64
+        (ss_energy_projected).  Uses the workspace's l buffers: not during a step."""
+        self._check(field)
+        out = ctypes.c_double()
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_energy_projected(self._h, _ptr(field), ctypes.byref(out)))
+        return out.value
+
     def energy_density(self, field, out=None):
         self._check(field)
         out = out if out is not None else torch.empty(self.N, dtype=torch.float64, device=self.device)

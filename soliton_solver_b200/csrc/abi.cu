@@ -572,6 +572,17 @@ struct Fused {
     return launch(h, A, tma);
   }
 
+  // FP64 energy of the sphere projection of `field` (element type R).  The FP64 copy
+  // goes to the start of the l-buffer region, which holds at least 8 * nf * N bytes
+  // for every precision (two FP32 l buffers, or one FP64 one) and is free between steps.
+  static int energy_projected(ss_handle* h, const void* field) {
+    double* copy = (double*)h->l[0];
+    project_kernel<R, TH::NF, TH::NMAG><<<grid_1d(h->G.N), 256, 0, h->stream>>>(
+        (const R*)field, copy, h->G.N, TH::CONSTRAINED && h->G.unit_mag);
+    CK(cudaGetLastError());
+    return Fused<TH, double>::energy(h, copy);
+  }
+
   static int density(ss_handle* h, const void* field, double* dens, bool reduce, int kind, int which) {
     auto k = density_kernel<TH, R, TX, TY, NT>;
     set_smem(k, BUF, smem_done_density);
@@ -983,6 +994,19 @@ int ss_energy(ss_handle* h, const void* field, double* out) {
     using TH = std::remove_pointer_t<decltype(tag)>;
     if (h->precision == SS_FP32) return Fused<TH, float>::energy(h, field);
     return Fused<TH, double>::energy(h, field);
+  });
+  if (rc) return rc;
+  return scalar_result(h, out);
+}
+
+int ss_energy_projected(ss_handle* h, const void* field, double* out) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!field || !out) return fail(SS_ERR_ARG, "NULL argument");
+  rc = dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (h->precision == SS_FP32) return Fused<TH, float>::energy_projected(h, field);
+    return Fused<TH, double>::energy_projected(h, field);
   });
   if (rc) return rc;
   return scalar_result(h, out);

@@ -955,4 +955,29 @@ __global__ void rk4_finalize_kernel(R* vel, R* phi, const R* k1, const R* k2, co
   }
 }
 
+// FP64 copy of a field with each site's unit-vector components divided by their
+// FP64 norm (the projection the flow applies after every step).  A stored FP32 unit
+// vector cannot hold m3 = 1 - |m_perp|^2/2 once |m_perp| < 2.4e-4: it rounds to 1 and
+// |m|^2 - 1 = |m_perp|^2 > 0 there; the copy restores the constraint to FP64 rounding.
+template <typename R, int NF, int NMAG>
+__global__ void project_kernel(const R* phi, double* out, long long N, int normalize) {
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < N; s += (long long)gridDim.x * blockDim.x) {
+    double P[NF];
+#pragma unroll
+    for (int a = 0; a < NF; ++a) P[a] = (double)phi[a * N + s];
+    if (NMAG > 0 && normalize) {
+      double s2 = 0.0;
+#pragma unroll
+      for (int a = 0; a < NMAG; ++a) s2 += P[a] * P[a];
+      if (s2 > 0.0) {
+        const double nrm = sqrt(s2);
+#pragma unroll
+        for (int a = 0; a < NMAG; ++a) P[a] /= nrm;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < NF; ++a) out[a * N + s] = P[a];
+  }
+}
+
 }  // namespace ssb

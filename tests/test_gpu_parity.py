@@ -199,6 +199,38 @@ def test_ragged_grids_vs_oracle(th, kw, prec):
     np.testing.assert_allclose(E, E_w, rtol=1e-11 if prec == "fp64" else 1e-5)
 
 
+PROJ = [BIG[0], BIG[1], BIG[4], BIG[5], BIG[6], BIG[8]]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64", "plain_fp64"])
+@pytest.mark.parametrize("th,kw", PROJ, ids=[f"{t}-{k['xlen']}x{k['ylen']}" for t, k in PROJ])
+def test_projected_energy_vs_oracle(th, kw, prec):
+    """ss_energy_projected = the oracle's FP64 energy of the stored values with each
+    site's unit vector renormalised in FP64 (the fields carry 1e-3 noise off the sphere,
+    so the projection is visible); identity for theories without the constraint."""
+    theory = load_theory(NAMES[th])
+    rp = theory.params.default_params(**kw).resolved()
+    p_i, p_f = theory.params.pack_device_params(rp)
+    F = _cast(_smooth_field(th, rp, 11), prec)
+    Fo = ref.as_field(F, p_i)
+    nmag = 3 if th in ("chiral_magnet", "baby_skyrme") else 0
+    want = ref.energy(th, ref.normalize_magnetization(Fo, nmag), p_i, p_f)
+    s = Solver(theory.kernels.THEORY_ID, p_i, p_f, prec)
+    f = _dev(F, prec)
+    s.bind(f, torch.zeros_like(f))
+    _rel(s.energy_projected(f), want, 1e-10, "projected energy")
+    raw = ref.energy(th, Fo, p_i, p_f)
+    if nmag:
+        assert abs(want - raw) > 1e-6 * abs(raw)   # the projection changed the energy
+    else:
+        assert want == raw
+    # FP64 fields on the sphere: the projection moves nothing beyond rounding
+    if prec != "fp32" and nmag:
+        U = ref.normalize_magnetization(Fo, nmag)
+        u = _dev(U, prec)
+        _rel(s.energy_projected(u), s.energy(u), 1e-13, "projected vs plain energy on the sphere")
+
+
 def test_step_chunking_is_bitwise_invariant():
     """Ten steps in one call equal 3 + 7 steps: the fused energy of the next stage 1
     and the trailing energy pass use the same tiles and the same reduction order."""
