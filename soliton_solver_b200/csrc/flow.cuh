@@ -104,12 +104,15 @@ __device__ inline void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
+// try_wait with a suspend-time hint: the thread sleeps until the phase completes or
+// ~1 ms passes instead of spinning, so waiting warps take no issue slots from the
+// warps that compute.
 __device__ inline bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(1000000u)
       : "memory");
   return ok != 0;
 }
@@ -393,21 +396,45 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
   if (MODE == M_S4) err_max = fmax(err_max, (double)emax);
 }
 
+// Stored value -> FP64 for the energy stencil.  For FP32 the float's bits are placed
+// in a double without re-biasing the exponent (two ALU ops and a shift instead of an
+// F2F conversion, which issues on the narrow XU pipe): the result is x * 2^-896
+// exactly for zero, normal and subnormal x (2^-126 * 2^-896 = 2^-1022, the smallest
+// normal double).  Derivative coefficients carry the factor 2^896 back and centre
+// values are multiplied by it, both exact, so every derivative and density is
+// bitwise what an F2F conversion gives.  Inf/NaN map to finite values here; the
+// caller folds v * 0 of every centre value into a sentinel instead.
+template <typename E>
+struct ScaledValue {
+  static constexpr double SCALE = 1.0;
+  __device__ static __forceinline__ double get(E x) { return (double)x; }
+};
+template <>
+struct ScaledValue<float> {
+  static constexpr double SCALE = 0x1p896;
+  __device__ static __forceinline__ double get(float x) {
+    const int u = __float_as_int(x);
+    return __hiloint2double((u >> 3) & (int)0x8fffffff, u << 29);
+  }
+};
+
 // FP64 energy of the staged field (T_1 = phi): first derivatives from the exact
 // differences f(x+k) - f(x-k) of the stored values, evaluated in FP64.
 template <class TH, typename R, int TX, int TY, int NT, bool FAST, typename E = R>
 __device__ __forceinline__ double energy_tile(const FlowArgs<R>& A, const E* T, int x0, int y0) {
   using TS = TileShape<TX, TY, NT>;
   using V = typename PairOf<E>::type;
+  using SV = ScaledValue<E>;
   constexpr int NF = TH::NF;
   constexpr int PAIRS = TY / 2;
   constexpr int RPP = NT / PAIRS;
   const Grid& G = A.G;
-  const double c23x = FD::c23 * G.ihx, c12x = FD::c12 * G.ihx;
-  const double c23y = FD::c23 * G.ihy, c12y = FD::c12 * G.ihy;
+  const double c23x = FD::c23 * G.ihx * SV::SCALE, c12x = FD::c12 * G.ihx * SV::SCALE;
+  const double c23y = FD::c23 * G.ihy * SV::SCALE, c12y = FD::c12 * G.ihy * SV::SCALE;
   const int j = threadIdx.x % PAIRS;
   const int lxg = threadIdx.x / PAIRS;
   double e_acc = 0.0;
+  V chk(0.0f);  // stays zero unless a centre value is Inf or NaN
 #pragma unroll 1
   for (int pass = 0; pass < TX / RPP; ++pass) {
     const int lx = lxg + pass * RPP;
@@ -427,19 +454,20 @@ __device__ __forceinline__ double energy_tile(const FlowArgs<R>& A, const E* T, 
       const E* row = T + a * TS::PLANE + toff;
       // six y values cover both sites' y stencils; converted once
       const V Ap = ld_pair(row - 2), B = ld_pair(row), C = ld_pair(row + 2);
-      const double y_2 = (double)Lanes<V>::get(Ap, 0), y_1 = (double)Lanes<V>::get(Ap, 1);
-      const double y0v = (double)Lanes<V>::get(B, 0), y1v = (double)Lanes<V>::get(B, 1);
-      const double y2 = (double)Lanes<V>::get(C, 0), y3 = (double)Lanes<V>::get(C, 1);
+      chk = vfma(B, V(0.0f), chk);
+      const double y_2 = SV::get(Lanes<V>::get(Ap, 0)), y_1 = SV::get(Lanes<V>::get(Ap, 1));
+      const double y0v = SV::get(Lanes<V>::get(B, 0)), y1v = SV::get(Lanes<V>::get(B, 1));
+      const double y2 = SV::get(Lanes<V>::get(C, 0)), y3 = SV::get(Lanes<V>::get(C, 1));
       const V xp1 = ld_pair(row + TS::HY), xm1 = ld_pair(row - TS::HY);
       const V xp2 = ld_pair(row + 2 * TS::HY), xm2 = ld_pair(row - 2 * TS::HY);
 #pragma unroll
       for (int l = 0; l < 2; ++l) {
         Jet1<double, NF>& J = l ? J1 : J0;
         const Masks& m = l ? m1 : m0;
-        const double ddx = (c23x * ((double)Lanes<V>::get(xp1, l) - (double)Lanes<V>::get(xm1, l)) -
-                            c12x * ((double)Lanes<V>::get(xp2, l) - (double)Lanes<V>::get(xm2, l)));
+        const double ddx = (c23x * (SV::get(Lanes<V>::get(xp1, l)) - SV::get(Lanes<V>::get(xm1, l))) -
+                            c12x * (SV::get(Lanes<V>::get(xp2, l)) - SV::get(Lanes<V>::get(xm2, l))));
         const double ddy = l ? (c23y * (y2 - y0v) - c12y * (y3 - y_1)) : (c23y * (y1v - y_1) - c12y * (y2 - y_2));
-        J.f[a] = l ? y1v : y0v;
+        J.f[a] = (l ? y1v : y0v) * SV::SCALE;
         J.dx[a] = m.x ? ddx : 0.0;
         J.dy[a] = m.y ? ddy : 0.0;
       }
@@ -447,7 +475,7 @@ __device__ __forceinline__ double energy_tile(const FlowArgs<R>& A, const E* T, 
     e_acc += TH::energy(J0, A.P, G.dA);
     if (v1) e_acc += TH::energy(J1, A.P, G.dA);
   }
-  return e_acc;
+  return e_acc + (double)(Lanes<V>::get(chk, 0) + Lanes<V>::get(chk, 1));
 }
 
 // Shared scratch of the one-tile-per-CTA stage kernels besides the staged tile.
