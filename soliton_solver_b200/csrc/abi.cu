@@ -563,9 +563,11 @@ struct Fused {
     return launch(h, A, tma);
   }
 
+  // the observable: exact FP64 stencil of the stored values for every precision
   static int energy(ss_handle* h, const void* field) {
     FlowArgs<R> A = base_args(h);
     A.mode = M_ENERGY;
+    A.exact_energy = 1;
     A.phi = (const R*)field;
     A.with_energy = 1;
     const bool tma = encode_tile_map(&A.tm_phi, field, sizeof(R), h->G.X, h->G.Y, TH::NF);
@@ -1136,6 +1138,7 @@ extern "C" int ss_energy_noalloc(int theory, const int32_t* p_i, int n_i, const 
     if (precision == SS_FP32) {
       FlowArgs<float> A = Fused<TH, float>::base_args(&h);
       A.mode = M_ENERGY;
+      A.exact_energy = 1;
       A.phi = (const float*)field;
       A.with_energy = 1;
       return Fused<TH, float>::template launch_mode<false, M_ENERGY>(&h, A);

@@ -71,6 +71,7 @@ __global__ void __launch_bounds__(NT)
     A.init_state = B.init_state;
     A.prev_energy = B.prev_energy ? B.prev_energy[inst] : NAN;
     A.grad_raw = 0;
+    A.exact_energy = 0;
     A.wait_cycles = B.wait_cycles;
     A.tx_extra = 0;
   }

@@ -63,6 +63,8 @@ struct FlowArgs {
   int init_state;     // first S1 of a call: arrest = 0 and (unless NaN) E_last = prev_energy
   double prev_energy;
   int grad_raw;           // M_GRAD: unprojected, not halo-zeroed dE/dphi with true saddle rows
+  int exact_energy;       // M_ENERGY on FP32 fields: 1 = FP64 stencil of the stored values
+                          // (observables), 0 = from the FP32 jets like stage 1 (flow energies)
   long long wait_cycles;  // bound of every mbarrier wait (clock64 cycles)
   unsigned tx_extra;      // test hook: bytes the barrier expects beyond what is loaded (normally 0)
   Grid G;
@@ -257,13 +259,63 @@ __device__ __forceinline__ void gstore(R* p, V v, bool fast, bool v1) {
   if (v1) p[1] = Lanes<V>::get(v, 1);
 }
 
+// Stored value -> FP64 for the energy stencil.  For FP32 the float's bits are placed
+// in a double without re-biasing the exponent (two ALU ops and a shift instead of an
+// F2F conversion, which issues on the narrow XU pipe): the result is x * 2^-896
+// exactly for zero, normal and subnormal x (2^-126 * 2^-896 = 2^-1022, the smallest
+// normal double).  Derivative coefficients carry the factor 2^896 back and centre
+// values are multiplied by it, both exact, so every derivative and density is
+// bitwise what an F2F conversion gives.  Inf/NaN map to finite values here; the
+// caller folds v * 0 of every centre value into a sentinel instead.
+template <typename E>
+struct ScaledValue {
+  static constexpr double SCALE = 1.0;
+  __device__ static __forceinline__ double get(E x) { return (double)x; }
+};
+template <>
+struct ScaledValue<float> {
+  static constexpr double SCALE = 0x1p896;
+  __device__ static __forceinline__ double get(float x) {
+    const int u = __float_as_int(x);
+    return __hiloint2double((u >> 3) & (int)0x8fffffff, u << 29);
+  }
+};
+
+// FP64 energy of an FP32 site pair from the jets the gradient stencil already built
+// (f, dx, dy after masking): the theory's energy point evaluated in FP64 on the
+// converted jets, so a flow stage pays no second stencil for its energy.  The jets
+// carry FP32 rounding (~1e-7 relative per site), the precision the flow's gradient
+// has.  `chk` folds v * 0 of every jet value (Inf/NaN -> NaN, see ScaledValue).
+template <class TH, typename V, int NF>
+__device__ __forceinline__ double jet_energy(const Jet<V, NF>& J, const Phys& P, double dA, bool v1, V& chk) {
+  using SV = ScaledValue<float>;
+  Jet1<double, NF> J0, J1;
+#pragma unroll
+  for (int a = 0; a < NF; ++a) {
+    chk = vfma(J.f[a], V(0.0f), chk);
+    chk = vfma(J.dx[a], V(0.0f), chk);
+    chk = vfma(J.dy[a], V(0.0f), chk);
+    J0.f[a] = SV::get(Lanes<V>::get(J.f[a], 0)) * SV::SCALE;
+    J1.f[a] = SV::get(Lanes<V>::get(J.f[a], 1)) * SV::SCALE;
+    J0.dx[a] = SV::get(Lanes<V>::get(J.dx[a], 0)) * SV::SCALE;
+    J1.dx[a] = SV::get(Lanes<V>::get(J.dx[a], 1)) * SV::SCALE;
+    J0.dy[a] = SV::get(Lanes<V>::get(J.dy[a], 0)) * SV::SCALE;
+    J1.dy[a] = SV::get(Lanes<V>::get(J.dy[a], 1)) * SV::SCALE;
+  }
+  double e = TH::energy(J0, P, dA);
+  if (v1) e += TH::energy(J1, P, dA);
+  return e;
+}
+
 // The per-site work of one staged tile.  Each thread owns y-adjacent site pairs;
 // FAST: the tile is interior (every derivative mask true, no halo site) and the
 // lattice row length is even, so pairs are aligned and need no lane masks.
-template <class TH, typename R, int TX, int TY, int NT, bool FAST, int MODE>
+// JE (FP32 stage 1 and the energy pass): add the energy of the jets to *e_acc (when
+// non-null); in M_ENERGY the gradient itself is skipped.
+template <class TH, typename R, int TX, int TY, int NT, bool FAST, int MODE, bool JE = false>
 __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, const R* Praw, const R* Vraw, int x0,
                                           int y0, bool arrest, double& err_max, const R* C1 = nullptr,
-                                          const R* C3 = nullptr) {
+                                          const R* C3 = nullptr, double* e_acc = nullptr) {
   using TS = TileShape<TX, TY, NT>;
   using V = typename PairOf<R>::type;
   constexpr int NF = TH::NF;
@@ -276,6 +328,8 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
   const PairCoef<V> kc(G);
   const V mdt(grid_k<S>(G, GK_MDT));
   S emax = -INFINITY;
+  V chk(0.0);
+  double e_pair = 0.0;
   const int j = threadIdx.x % PAIRS;
   const int lxg = threadIdx.x / PAIRS;
 #pragma unroll 1
@@ -308,6 +362,19 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
         J.dxy[a] = mask_lanes(J.dxy[a], m0.xy, m1.xy);
       }
     }
+    if constexpr (JE) {
+      if (e_acc) {
+        if constexpr (TH::PAIR_ENERGY) {
+          // energy point in packed FP32; F2F keeps Inf/NaN
+          const V ep = TH::energy_pair(J, A.P);
+          e_pair += (double)Lanes<V>::get(ep, 0);
+          if (v1) e_pair += (double)Lanes<V>::get(ep, 1);
+        } else {
+          *e_acc += jet_energy<TH, V, NF>(J, A.P, G.dA, v1, chk);
+        }
+      }
+    }
+    if constexpr (MODE == M_ENERGY) continue;
 
     V g[NF];
     TH::gradient(J, A.P, g);
@@ -394,29 +461,10 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
     }
   }
   if (MODE == M_S4) err_max = fmax(err_max, (double)emax);
-}
-
-// Stored value -> FP64 for the energy stencil.  For FP32 the float's bits are placed
-// in a double without re-biasing the exponent (two ALU ops and a shift instead of an
-// F2F conversion, which issues on the narrow XU pipe): the result is x * 2^-896
-// exactly for zero, normal and subnormal x (2^-126 * 2^-896 = 2^-1022, the smallest
-// normal double).  Derivative coefficients carry the factor 2^896 back and centre
-// values are multiplied by it, both exact, so every derivative and density is
-// bitwise what an F2F conversion gives.  Inf/NaN map to finite values here; the
-// caller folds v * 0 of every centre value into a sentinel instead.
-template <typename E>
-struct ScaledValue {
-  static constexpr double SCALE = 1.0;
-  __device__ static __forceinline__ double get(E x) { return (double)x; }
-};
-template <>
-struct ScaledValue<float> {
-  static constexpr double SCALE = 0x1p896;
-  __device__ static __forceinline__ double get(float x) {
-    const int u = __float_as_int(x);
-    return __hiloint2double((u >> 3) & (int)0x8fffffff, u << 29);
+  if constexpr (JE) {
+    if (e_acc) *e_acc += e_pair * G.dA + (double)(Lanes<V>::get(chk, 0) + Lanes<V>::get(chk, 1));
   }
-};
+}
 
 // FP64 energy of the staged field (T_1 = phi): first derivatives from the exact
 // differences f(x+k) - f(x-k) of the stored values, evaluated in FP64.
@@ -584,20 +632,26 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   }
   const bool fast = (G.Y % 2 == 0) && x0 >= G.halo + 1 && x0 + TX - 1 <= G.X - G.halo - 2 && y0 >= G.halo + 1 &&
                     y0 + TY - 1 <= G.Y - G.halo - 2;
-  if constexpr (MODE != M_ENERGY) {
-    if (fast)
-      grad_tile<TH, R, TX, TY, NT, true, MODE>(A, T, Praw, Vraw, x0, y0, arrest, err_max);
-    else
-      grad_tile<TH, R, TX, TY, NT, false, MODE>(A, T, Praw, Vraw, x0, y0, arrest, err_max);
+  // FP32 fields: the energy comes from the gradient stencil's jets; FP64 fields: from
+  // exact FP64 differences of the staged values (energy_tile)
+  constexpr bool JE = sizeof(R) == 4 && (MODE == M_S1 || MODE == M_ENERGY);
+  const bool je = JE && !(MODE == M_ENERGY && A.exact_energy);
+  if constexpr (MODE != M_ENERGY || JE) {
+    if (MODE != M_ENERGY || je) {
+      double* ep = (je && do_energy) ? &e_acc : nullptr;
+      if (fast)
+        grad_tile<TH, R, TX, TY, NT, true, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, nullptr, nullptr, ep);
+      else
+        grad_tile<TH, R, TX, TY, NT, false, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, nullptr, nullptr,
+                                                     ep);
+    }
   }
   if constexpr (MODE == M_S1 || MODE == M_ENERGY) {
-    if (do_energy) {
-      {
-        if (fast)
-          e_acc = energy_tile<TH, R, TX, TY, NT, true>(A, T, x0, y0);
-        else
-          e_acc = energy_tile<TH, R, TX, TY, NT, false>(A, T, x0, y0);
-      }
+    if (do_energy && !je) {
+      if (fast)
+        e_acc = energy_tile<TH, R, TX, TY, NT, true>(A, T, x0, y0);
+      else
+        e_acc = energy_tile<TH, R, TX, TY, NT, false>(A, T, x0, y0);
     }
   }
 
@@ -788,14 +842,19 @@ __global__ void __launch_bounds__(NT, 1) flow_kernel_pipe(const __grid_constant_
     const R* C3 = MODE == M_S4 ? base + 3 * BUF + CBUF : nullptr;
     const bool fast = (G.Y % 2 == 0) && x0 >= G.halo + 1 && x0 + TX - 1 <= G.X - G.halo - 2 &&
                       y0 >= G.halo + 1 && y0 + TY - 1 <= G.Y - G.halo - 2;
-    if constexpr (MODE != M_ENERGY) {
-      if (fast)
-        grad_tile<TH, R, TX, TY, NT, true, MODE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3);
-      else
-        grad_tile<TH, R, TX, TY, NT, false, MODE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3);
+    constexpr bool JE = sizeof(R) == 4 && (MODE == M_S1 || MODE == M_ENERGY);
+    const bool je = JE && !(MODE == M_ENERGY && A.exact_energy);
+    if constexpr (MODE != M_ENERGY || JE) {
+      if (MODE != M_ENERGY || je) {
+        double* ep = (je && do_energy) ? &e_acc : nullptr;
+        if (fast)
+          grad_tile<TH, R, TX, TY, NT, true, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3, ep);
+        else
+          grad_tile<TH, R, TX, TY, NT, false, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3, ep);
+      }
     }
     if constexpr (MODE == M_S1 || MODE == M_ENERGY) {
-      if (do_energy) {
+      if (do_energy && !je) {
         if (fast)
           e_acc += energy_tile<TH, R, TX, TY, NT, true>(A, T, x0, y0);
         else

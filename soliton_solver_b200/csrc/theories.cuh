@@ -8,6 +8,8 @@
 //   NEED_XY          mixed derivatives used
 //   gradient<R>()    dE/dphi at one site in working precision R (before projection)
 //   energy()         energy density (FP64), already multiplied by dA
+//   PAIR_ENERGY      energy_pair<V>() exists: the energy point (without dA) of a packed
+//                    FP32 site pair, used for the flow's per-step energy in stage 1
 // plus the charge densities / coupling partials it supports.  Every function
 // states the reference lines it restates.
 #pragma once
@@ -42,7 +44,7 @@ __device__ inline double skyrmion_density(const Jet1<double, NF>& J, double dA) 
 // ===========================================================================
 struct ChiralMagnet {
   static constexpr int NF = 4, NMAG = 3;
-  static constexpr bool CONSTRAINED = true, HALO_ZERO = true, NEED_XY = false;
+  static constexpr bool CONSTRAINED = true, HALO_ZERO = true, NEED_XY = false, PAIR_ENERGY = true;
 
   // do_gradient_step_point, kernels.py:398-503 (halo zeroing and projection are
   // applied by the caller, kernels.py:505-511).  Constants are pre-scaled so every
@@ -118,6 +120,33 @@ struct ChiralMagnet {
     return e * dA;
   }
 
+  // The same energy point (without dA) in the stage's own arithmetic, for a packed
+  // FP32 site pair of jets: the flow's per-step energy in stage 1.
+  template <typename V>
+  __device__ static inline V energy_pair(const Jet<V, NF>& J, const Phys& P) {
+    const double D00 = P.c[3], D01 = P.c[4], D10 = P.c[5], D11 = P.c[6];
+    V q = J.dx[0] * J.dx[0];
+    q = vfma(J.dx[1], J.dx[1], q);
+    q = vfma(J.dx[2], J.dx[2], q);
+    q = vfma(J.dy[0], J.dy[0], q);
+    q = vfma(J.dy[1], J.dy[1], q);
+    q = vfma(J.dy[2], J.dy[2], q);
+    V e = q * V(0.5f);
+    const V* m = J.f;
+    if (D00 != 0.0) e = vfma(pk<V>(P, 3), vfma(m[1], J.dx[2], -(m[2] * J.dx[1])), e);
+    if (D10 != 0.0) e = vfma(pk<V>(P, 5), vfma(m[2], J.dx[0], -(m[0] * J.dx[2])), e);
+    if (D01 != 0.0) e = vfma(pk<V>(P, 4), vfma(m[1], J.dy[2], -(m[2] * J.dy[1])), e);
+    if (D11 != 0.0) e = vfma(pk<V>(P, 6), vfma(m[2], J.dy[0], -(m[0] * J.dy[2])), e);
+    if (P.k[0]) {
+      const V g2 = vfma(J.dx[3], J.dx[3], J.dy[3] * J.dy[3]);
+      e = e - vfma(m[3], J.dx[0] + J.dy[1], g2 * pk<V>(P, 21));
+    }
+    const V one(1.0f);
+    e = vfma(pk<V>(P, 1), one - m[2], e);
+    e = vfma(pk<V>(P, 0), vfma(-m[2], m[2], one), e);
+    return e;
+  }
+
   __device__ static inline double charge(const Jet1<double, NF>& J, const Phys&, int which, double dA) {
     if (which == CH_SKYRMION) return skyrmion_density<NF>(J, dA);
     // compute_magnetic_charge_point, kernels.py:329-360
@@ -149,7 +178,7 @@ struct ChiralMagnet {
 // ===========================================================================
 struct BabySkyrme {
   static constexpr int NF = 3, NMAG = 3;
-  static constexpr bool CONSTRAINED = true, HALO_ZERO = false, NEED_XY = true;
+  static constexpr bool CONSTRAINED = true, HALO_ZERO = false, NEED_XY = true, PAIR_ENERGY = false;
   template <typename R>
   __device__ static inline void true_rows(R*, const Phys&) {}
 
@@ -331,7 +360,7 @@ struct BabySkyrme {
 // ===========================================================================
 struct GinzburgLandau {
   static constexpr int NF = 4, NMAG = 0;
-  static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true;
+  static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true, PAIR_ENERGY = false;
   template <typename R>
   __device__ static inline void true_rows(R*, const Phys&) {}
 
@@ -400,7 +429,7 @@ struct GinzburgLandau {
 // ===========================================================================
 struct Anisotropic {
   static constexpr int NF = 6, NMAG = 0;
-  static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true;
+  static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true, PAIR_ENERGY = false;
   template <typename R>
   __device__ static inline void true_rows(R*, const Phys&) {}
 

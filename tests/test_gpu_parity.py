@@ -257,6 +257,37 @@ def test_step_chunking_is_bitwise_invariant():
         np.testing.assert_array_equal(v, outs[0][2])
 
 
+FLOW_E = [("chiral_magnet", dict(xlen=150, ylen=140, xsize=10.0, ysize=10.0, dmi_term="Heusler", demag=True,
+                                 unit_magnetization=True)),
+          ("baby_skyrme", dict(xlen=70, ylen=128, xsize=7.0, ysize=13.0, kappa=1.0, mpi=1.0, time_step=0.01,
+                               unit_magnetization=True)),
+          ("ginzburg_landau_superconductor", dict(xlen=96, ylen=132, xsize=8.0, ysize=10.0, Lambda=0.5))]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("th,kw", FLOW_E, ids=[t for t, _ in FLOW_E])
+def test_flow_energy_vs_observable(th, kw, prec):
+    """The flow's per-step energy (stage 1 and the trailing pass) against the energy
+    observable of the same field.  FP64 fields: one code path, bitwise equal.  FP32
+    fields: the flow evaluates the energy point on the gradient stencil's FP32 jets
+    (packed FP32 for the chiral magnet, FP64 on converted jets otherwise) while the
+    observable is the FP64 stencil of the stored values; both reduce in FP64."""
+    theory = load_theory(NAMES[th])
+    rp = theory.params.default_params(**kw).resolved()
+    p_i, p_f = theory.params.pack_device_params(rp)
+    F = _cast(_smooth_field(th, rp, 5), prec)
+    s = Solver(theory.kernels.THEORY_ID, p_i, p_f, prec)
+    f, v = _dev(F, prec), _dev(np.zeros_like(F), prec)
+    s.bind(f, v)
+    E, _ = s.step(4, 1e300)
+    obs = s.energy(f)
+    if prec == "fp64":
+        assert E[-1] == obs
+    else:
+        _rel(E[-1], obs, 1e-6, "flow energy vs observable")
+        _rel(obs, ref.energy(th, ref.as_field(f.double().cpu().numpy(), p_i), p_i, p_f), 1e-10, "observable")
+
+
 def test_arrest_matches_oracle_fp64():
     """Start with a large velocity so that the energy rises and arrest fires."""
     theory = load_theory("Baby Skyrme")
