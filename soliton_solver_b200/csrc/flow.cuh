@@ -315,7 +315,8 @@ __device__ __forceinline__ double jet_energy(const Jet<V, NF>& J, const Phys& P,
 template <class TH, typename R, int TX, int TY, int NT, bool FAST, int MODE, bool JE = false>
 __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, const R* Praw, const R* Vraw, int x0,
                                           int y0, bool arrest, double& err_max, const R* C1 = nullptr,
-                                          const R* C3 = nullptr, double* e_acc = nullptr) {
+                                          const R* C3 = nullptr, double* e_acc = nullptr,
+                                          const typename PairOf<R>::type* L2c = nullptr) {
   using TS = TileShape<TX, TY, NT>;
   using V = typename PairOf<R>::type;
   constexpr int NF = TH::NF;
@@ -425,7 +426,7 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
         const V v = arrest ? V(0.0) : (Vraw ? ld_pair(Vraw + a * TS::PLANE + toff) : gload<V, R>(A.vel + idx, FAST, v1));
         const int coff = a * TX * TY + lx * TY + 2 * j;
         const V l1 = C1 ? ld_pair(C1 + coff) : gload<V, R>(A.la + idx, FAST, v1);
-        const V l2 = gload<V, R>(A.lb + idx, FAST, v1);
+        const V l2 = L2c ? L2c[a] : gload<V, R>(A.lb + idx, FAST, v1);
         const V l3 = C3 ? ld_pair(C3 + coff) : gload<V, R>(A.lc + idx, FAST, v1);
         const V l4 = mdt * g[a];
         Vn[a] = vfma(sixth, vfma(two, l3, vfma(two, l2, l1)) + l4, v);
@@ -559,7 +560,10 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   const int x0 = (tile / tiles_y) * TX;
   const int y0 = (tile % tiles_y) * TY;
   StepState* st = A.st;
-  const bool arrest = (mode == M_S2 || mode == M_S3 || mode == M_S4) && (st->arrest != 0);
+  constexpr bool uses_v = mode == M_S2 || mode == M_S3 || mode == M_S4;
+  // The arrest flag (set by the last block of stage 1) is read only after the TMA
+  // copies are issued, so its global-memory round trip overlaps them.
+  bool arrest = false;
   const bool do_energy = (MODE == M_S1 || MODE == M_ENERGY) && A.with_energy != 0;
 
   if (A.init_state && tile == 0 && threadIdx.x == 0) {
@@ -570,7 +574,8 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   // ---- stage the halo tile of T_s --------------------------------------
   R* T = B0;
   if constexpr (TMA) {
-    const bool need_v = (mode == M_S2 || mode == M_S3 || mode == M_S4) && !arrest;
+    // V is staged whether or not an arrest is pending (an arrested step ignores it)
+    constexpr bool need_v = uses_v;
     const bool need_l = mode == M_S3 || mode == M_S4;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
@@ -581,6 +586,7 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
       if (need_v) tma_load_3d(B1, tm_vel, y0 - TS::YOFF, x0 - 2, 0, &bar);
       if (need_l) tma_load_3d(B2, tm_l, y0 - TS::YOFF, x0 - 2, 0, &bar);
     }
+    if constexpr (uses_v) arrest = st->arrest != 0;
     const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0, A.wait_cycles));
     if (!ok) {
       if (threadIdx.x == 0) atomicExch(&st->status, (int)ST_TIMEOUT);
@@ -596,7 +602,7 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
         for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
           V p0, p1, v0(0.0), v1(0.0), w0(0.0), w1(0.0);
           ld_quad(B0 + i, p0, p1);
-          if (need_v) ld_quad(B1 + i, v0, v1);
+          if (need_v && !arrest) ld_quad(B1 + i, v0, v1);
           if (need_l) ld_quad(B2 + i, w0, w1);
           V t0, t1;
           if (mode == M_S2) {
@@ -616,6 +622,7 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
       T = dst;
     }
   } else {
+    if constexpr (uses_v) arrest = st->arrest != 0;
     stage_plain<NF, R, TX, TY, NT>(B0, A, x0, y0, mode, arrest);
     __syncthreads();
   }
@@ -809,6 +816,18 @@ __global__ void __launch_bounds__(NT, 1) flow_kernel_pipe(const __grid_constant_
       ++tx;
     }
     R* T = B0;
+    // Stage 4 combines T4 into the staged l2 tile in place, but the finalize needs l2
+    // at the thread's own sites: keep that pair in registers (one pass per thread)
+    // instead of re-reading it from global memory.
+    using VP = typename PairOf<R>::type;
+    constexpr bool L2REG = MODE == M_S4 && TX * (TY / 2) == NT;
+    VP l2c[L2REG ? NF : 1];
+    if constexpr (L2REG) {
+      const int toff = (threadIdx.x / (TY / 2) + 2) * TS::HY + TS::YOFF + 2 * (threadIdx.x % (TY / 2));
+#pragma unroll
+      for (int a = 0; a < NF; ++a) l2c[a] = ld_pair(B2 + a * TS::PLANE + toff);
+      __syncthreads();  // every pair is read before the combine overwrites the tile
+    }
     if (MODE == M_S2 || MODE == M_S3 || MODE == M_S4) {
       R* dst = need_l ? B2 : (need_v ? B1 : B0);
       if (dst != B0) {
@@ -848,9 +867,11 @@ __global__ void __launch_bounds__(NT, 1) flow_kernel_pipe(const __grid_constant_
       if (MODE != M_ENERGY || je) {
         double* ep = (je && do_energy) ? &e_acc : nullptr;
         if (fast)
-          grad_tile<TH, R, TX, TY, NT, true, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3, ep);
+          grad_tile<TH, R, TX, TY, NT, true, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3, ep,
+                                                      L2REG ? l2c : nullptr);
         else
-          grad_tile<TH, R, TX, TY, NT, false, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3, ep);
+          grad_tile<TH, R, TX, TY, NT, false, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3, ep,
+                                                       L2REG ? l2c : nullptr);
       }
     }
     if constexpr (MODE == M_S1 || MODE == M_ENERGY) {
