@@ -343,7 +343,8 @@ struct Fused {
   template <int MODE>
   static constexpr int pipe_stages() {
     const size_t slot = pipe_slot_bytes<R, TH::NF, TX, TY, MODE>();
-    const size_t budget = 212 * 1024;  // dynamic shared memory left next to the static reduction arrays
+    // dynamic shared memory left next to the static reduction arrays, per resident CTA
+    const size_t budget = pipe_ctas<TH, MODE>() == 2 ? 100 * 1024 : 212 * 1024;
     const int n = (int)(budget / slot);
     return n > 4 ? 4 : n;
   }
@@ -360,7 +361,7 @@ struct Fused {
       auto k = flow_kernel_pipe<TH, R, TX, TY, PIPE_NT, MODE, S>;
       const size_t smem = S * pipe_slot_bytes<R, TH::NF, TX, TY, MODE>();
       set_smem(k, smem, smem_done_pipe[MODE]);
-      const int grid = std::min(h->nblocks, h->num_sms);
+      const int grid = std::min(h->nblocks, pipe_ctas<TH, MODE>() * h->num_sms);
       k<<<grid, PIPE_NT, smem, h->stream>>>(A);
       CK(cudaGetLastError());
       return SS_OK;

@@ -730,8 +730,16 @@ __host__ __device__ constexpr size_t pipe_slot_bytes() {
          sizeof(R) * NF * TX * TY * pipe_centre_buffers<MODE>();
 }
 
+// Persistent CTAs per SM: two for stage 1 and the energy pass of a theory whose
+// energy point runs in packed FP32 (latency-bound, so twice the warps help), one
+// otherwise.  Stage 1 and the energy pass must agree: their partials are per CTA.
+template <class TH, int MODE>
+__host__ __device__ constexpr int pipe_ctas() {
+  return ((MODE == M_S1 || MODE == M_ENERGY) && TH::PAIR_ENERGY) ? 2 : 1;
+}
+
 template <class TH, typename R, int TX, int TY, int NT, int MODE, int STAGES>
-__global__ void __launch_bounds__(NT, 1) flow_kernel_pipe(const __grid_constant__ FlowArgs<R> A) {
+__global__ void __launch_bounds__(NT, (pipe_ctas<TH, MODE>())) flow_kernel_pipe(const __grid_constant__ FlowArgs<R> A) {
   using TS = TileShape<TX, TY, NT>;
   constexpr int NF = TH::NF;
   constexpr int BUF = NF * TS::PLANE;             // elements of one halo buffer
