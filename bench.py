@@ -207,6 +207,11 @@ def gpu_arm(args, rank, world, local_rank):
     err_traj = torch.empty(K, dtype=torch.float64, device=dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     tuning = s.autotune(5)
+    if args.variants:
+        # pinned staging variants (S1..S4), e.g. to profile the set a normal run picks
+        for m, v in enumerate(args.variants.split(","), start=1):
+            s.set_variant(m, int(v))
+        tuning = {m: (a, b, s._lib.ss_get_variant(s._h, m)) for m, (a, b, _) in tuning.items()}
     with Clocks(local_rank) as clk:
         # warm-up (untimed); also gives the clock sampler time to start
         s.step(max(W, 1), 1e300)
@@ -468,6 +473,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 / plain-FP64 comparison")
+    ap.add_argument("--variants", default="", help="pin the staging variant of stages 1-4 after autotuning "
+                                                    "(comma-separated, 0 one tile per CTA, 1 pipelined)")
     ap.add_argument("--size", type=int, default=4096, help="lattice edge (4096 is the workload; smaller sizes "
                                                              "are for profiler captures)")
     args = ap.parse_args()

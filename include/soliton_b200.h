@@ -116,6 +116,12 @@ int ss_tma_enabled(const ss_handle *h);
 int ss_autotune(ss_handle *h, int iters, float *ms_out);
 /* Variant chosen for a flow mode (0..5): 1 pipelined, 0 one tile per CTA, -1 bad args. */
 int ss_get_variant(const ss_handle *h, int mode);
+/* Pin the staging variant of a flow mode instead of autotuning it: mode 0 (gradient)
+ * or 1..4 (stages; stage 1 also sets the energy pass, whose per-CTA partials must
+ * match it), variant 0 (one tile per CTA) or 1 (pipelined; needs TMA-staged bound
+ * buffers and FP32 fields).  For reproducible runs and for profiling a known kernel
+ * set.  No reference counterpart (tuning control). */
+int ss_set_variant(ss_handle *h, int mode, int variant);
 /* Failure-detection hook.  Sets the bound (clock64 cycles, default 2e9) of every
  * device-side mbarrier wait of this handle's kernels; with inject != 0 the next
  * TMA-staged stage kernel's barrier expects 16 bytes more than its loads deliver,

@@ -81,6 +81,7 @@ _SIG = {
     "ss_tma_enabled": ([_P], _I),
     "ss_autotune": ([_P, _I, _P], _I),
     "ss_get_variant": ([_P, _I], _I),
+    "ss_set_variant": ([_P, _I, _I], _I),
     "ss_debug_wait_timeout": ([_P, ctypes.c_longlong, _I], _I),
     "ss_gradient": ([_P, _P, _P, _P], _I),
     "ss_energy_gradient": ([_P, _P, _P], _I),

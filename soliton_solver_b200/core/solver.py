@@ -146,6 +146,11 @@ class Solver:
         return {m: (float(ms[2 * m]), float(ms[2 * m + 1]), int(self._lib.ss_get_variant(self._h, m)))
                 for m in (1, 2, 3, 4)}
 
+    def set_variant(self, stage: int, variant: int):
+        """Pin the staging variant of flow mode `stage` (0 gradient, 1-4 stages):
+        0 one tile per CTA, 1 pipelined (see ss_set_variant)."""
+        nat.check(self._lib.ss_set_variant(self._h, int(stage), int(variant)))
+
     def debug_wait_timeout(self, wait_cycles: int, inject: bool):
         """Failure-detection hook: bound of the device waits; optionally make the next
         stage kernel's wait expire (see ss_debug_wait_timeout)."""

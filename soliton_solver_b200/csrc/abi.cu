@@ -900,6 +900,24 @@ int ss_get_variant(const ss_handle* h, int mode) {
   return h->use_pipe[mode];
 }
 
+int ss_set_variant(ss_handle* h, int mode, int variant) {
+  if (!h) return fail(SS_ERR_ARG, "NULL handle");
+  if (mode < 0 || mode > 4) return fail(SS_ERR_ARG, "mode %d: 0 (gradient) or 1..4 (stages); the energy pass follows stage 1", mode);
+  if (variant != 0 && variant != 1) return fail(SS_ERR_ARG, "variant %d: 0 (one tile per CTA) or 1 (pipelined)", variant);
+  if (h->precision == SS_PLAIN_FP64) return fail(SS_ERR_ARG, "the plain FP64 form has no staging variants");
+  if (variant == 1) {
+    if (!h->tma) return fail(SS_ERR_STATE, "the pipelined variant needs TMA-staged buffers (bind first; rows of 16-byte multiples)");
+    const bool ok = dispatch(h, [&](auto* tag) -> int {
+      using TH = std::remove_pointer_t<decltype(tag)>;
+      return h->precision == SS_FP32 ? Fused<TH, float>::uses_pipe(mode) : Fused<TH, double>::uses_pipe(mode);
+    }) != 0;
+    if (!ok) return fail(SS_ERR_ARG, "no pipelined variant of mode %d for this theory and precision", mode);
+  }
+  h->use_pipe[mode] = variant;
+  if (mode == M_S1) h->use_pipe[M_ENERGY] = variant;  // the energy pass reduces exactly like stage 1
+  return SS_OK;
+}
+
 int ss_step_async(ss_handle* h, int n_steps, double prev_energy, double* energy_traj_dev, double* err_traj_dev) {
   int rc = check_bound(h);
   if (rc) return rc;

@@ -5,8 +5,10 @@ Tolerances (written here, checked below):
     (same arithmetic as the reference up to association / FMA contraction).
   * FP32 fields: the gradient is compared with the FP64 oracle evaluated on the
     same (FP32-representable) field: norm-wise relative error <= 1e-5 (the
-    per-step gradient bound of the target), per-entry <= 1e-4 x max.  Energies and
-    charges are reduced in FP64 from the FP32 field: relative error <= 1e-10.
+    per-step gradient bound of the target), per-entry <= 1e-4 x max.  Energy and
+    charge observables are FP64 stencils of the FP32 values reduced in FP64: relative
+    error <= 1e-10.  The flow's per-step energies on FP32 fields are evaluated on the
+    FP32 gradient jets (reduced in FP64): relative error <= 1e-6 against the observable.
 """
 import glob
 import math
@@ -435,3 +437,34 @@ def test_bounded_wait_timeout_is_reported_and_recoverable():
     s.check_status()
     _, eg_w = ref.gradient_step("chiral_magnet", ref.as_field(_cast(F, "fp32"), p_i), p_i, p_f)
     _cmp(eg.cpu().numpy(), eg_w, "fp32", "gradient after recovery")
+
+
+def test_pinned_variants_agree():
+    """ss_set_variant: every stage pinned to one tile per CTA, then to the pipelined
+    variant; the per-site arithmetic is the same, so the fields agree bitwise and the
+    energies (per-tile vs per-CTA partials) to rounding.  Bad arguments are rejected."""
+    theory = load_theory("Chiral magnet")
+    rp = theory.params.default_params(xlen=256, ylen=192, xsize=10.0, ysize=7.5, dmi_term="Heusler", demag=True,
+                                      unit_magnetization=True, killkinen=False).resolved()
+    p_i, p_f = theory.params.pack_device_params(rp)
+    F = _smooth_field("chiral_magnet", rp, 9)
+    outs = []
+    for v in (0, 1):
+        s = Solver(0, p_i, p_f, "fp32")
+        f, vel = _dev(F, "fp32"), _dev(np.zeros_like(F), "fp32")
+        s.bind(f, vel)
+        for m in (1, 2, 3, 4):
+            s.set_variant(m, v)
+            assert s._lib.ss_get_variant(s._h, m) == v
+        assert s._lib.ss_get_variant(s._h, 5) == v  # the energy pass follows stage 1
+        E, _ = s.step(6, 1e300)
+        outs.append((E, f.cpu().numpy(), vel.cpu().numpy()))
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+    np.testing.assert_array_equal(outs[0][2], outs[1][2])
+    np.testing.assert_allclose(outs[0][0], outs[1][0], rtol=1e-12)
+    for bad in ((5, 0), (1, 2), (-1, 0)):
+        with pytest.raises(ValueError):
+            s.set_variant(*bad)
+    sp = Solver(0, p_i, p_f, "plain_fp64")
+    with pytest.raises(ValueError):
+        sp.set_variant(1, 0)
