@@ -436,6 +436,54 @@ def small_lattice_graph(dev, steps=2000, chunk=100):
     return out
 
 
+def render_rgba(dev, F0, reps=20):
+    """Headless magnetisation colormap (ss_render_rgba) of the workload's 4096^2 FP32
+    field: 12 B read + 4 B written per pixel; CUDA events around `reps` launches."""
+    import torch
+    from soliton_solver_b200.core import colormaps as cm
+    F = F0.to(device=dev, dtype=torch.float32).contiguous()
+    out = torch.empty((YLEN, XLEN, 4), dtype=torch.uint8, device=dev)
+    p_i = np.array([XLEN, YLEN], dtype=np.int32)
+    for _ in range(3):
+        cm.render_magnetization_to_rgba[None, None](out, F, XLEN, YLEN, p_i)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        cm.render_magnetization_to_rgba[None, None](out, F, XLEN, YLEN, p_i)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    us = e0.elapsed_time(e1) / reps * 1e3
+    gbs = XLEN * YLEN * 16 / (us * 1e-6) / 1e9
+    peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0)) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    return {"kernel": "render_kernel<float, magnetization> (ss_render_rgba)", "pixels": XLEN * YLEN,
+            "us_per_image": us, "achieved_gbs": gbs, "frac": gbs / peak, "bytes_per_pixel": 16}
+
+
+def initial_condition(dev, reps=10):
+    """The chiral magnet's skyrmion ansatz (ss_initialize) written into a 4096^2 FP32
+    field and velocity: 8 words written per site, FP64 sin/cos/exp/atan2 per site."""
+    import torch
+    from soliton_solver_b200 import _native as nat
+    from soliton_solver_b200.core.simulation import Simulation
+    th, p = chiral_params()
+    sim = Simulation(p, th, precision="fp32", device=dev)
+    s = sim.solver
+    for _ in range(2):
+        s.initialize(sim.Field, sim.Velocity, nat.SS_INIT_ANSATZ, nat.SS_ANSATZ_ANTI, 0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        s.initialize(sim.Field, sim.Velocity, nat.SS_INIT_ANSATZ, nat.SS_ANSATZ_ANTI, 0.3)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    us = e0.elapsed_time(e1) / reps * 1e3
+    del sim
+    torch.cuda.empty_cache()
+    return {"kernel": "init_kernel<chiral, float> (ss_initialize, anti-skyrmion ansatz)", "sites": XLEN * YLEN,
+            "us": us, "achieved_gbs": XLEN * YLEN * 32 / (us * 1e-6) / 1e9, "bytes_per_site": 32}
+
+
 def compare_fp64_and_plain(args, dev, F0):
     """Relaxed-state accuracy (320^2), and the plain-FP64 form's speed on this lattice."""
     import torch
@@ -443,7 +491,8 @@ def compare_fp64_and_plain(args, dev, F0):
     th, p = chiral_params()
     out = {}
     for key, fn in (("accuracy", relaxed_accuracy), ("batched_sweep", batched_sweep),
-                    ("graph_320", small_lattice_graph)):
+                    ("graph_320", small_lattice_graph), ("render_rgba", lambda d: render_rgba(d, F0)),
+                    ("initial_condition", initial_condition)):
         try:
             out[key] = fn(dev)
         except Exception as exc:  # reported, not fatal: the headline line must still print

@@ -72,6 +72,19 @@ extern "C" {
 #define SS_COUPLING_COUP_H 4  /* chiral magnet coup_h (p_f[7]) */
 #define SS_COUPLING_COUP_MU 5 /* chiral magnet coup_mu (p_f[8]) */
 
+/* colormaps for ss_render_rgba */
+#define SS_RENDER_JET 0           /* core/colormaps.py render_jet_density_to_rgba */
+#define SS_RENDER_GRAY 1          /* core/colormaps.py render_gray_density_to_rgba */
+#define SS_RENDER_MAGNETIZATION 2 /* core/colormaps.py render_magnetization_to_rgba */
+
+/* initial conditions (ss_initialize, ss_insert_soliton) */
+#define SS_INIT_GROUND 0   /* create_ground_state_kernel */
+#define SS_INIT_ANSATZ 1   /* create_initial_configuration_kernel */
+#define SS_ANSATZ_NONE 0   /* chiral magnet / baby Skyrme ansatz flags (ansatz_bloch, ansatz_neel, ansatz_anti) */
+#define SS_ANSATZ_BLOCH 1
+#define SS_ANSATZ_NEEL 2
+#define SS_ANSATZ_ANTI 3
+
 typedef struct ss_handle ss_handle;
 typedef struct ss_batch ss_batch;
 
@@ -156,6 +169,42 @@ int ss_energy(ss_handle *h, const void *field, double *out);
  * unit-vector constraint it equals the FP64 energy of the field.  Uses the l-buffer
  * part of the bound workspace.  No reference counterpart (new observable). */
 int ss_energy_projected(ss_handle *h, const void *field, double *out);
+
+/* Initial configuration of the handle's theory into field (and velocity, nullable:
+ * set to zero), element type of the handle, on the bound stream (asynchronous).
+ * SS_INIT_GROUND: the vacuum of create_ground_state_kernel.  SS_INIT_ANSATZ: the
+ * single soliton of create_initial_configuration_kernel at the lattice centre —
+ * chiral magnet / baby Skyrme: `ansatz` (SS_ANSATZ_*) rotated by `rotation`, with the
+ * skyrmion number of the packed params; Abelian Higgs: winding `vortex_number`; s+id:
+ * the packed windings.  Reference quirks kept: the s+id ground state reads u1, u2 from
+ * p_f[11], p_f[12]; one bug repaired: the Abelian Higgs ansatz reads ainf from its packed
+ * slot p_f[10] (the reference reads one past the array).  Replaces
+ * theories/<theory>/initial_config.py create_ground_state_kernel and
+ * create_initial_configuration_kernel (e.g. chiral_magnet/initial_config.py:117-283);
+ * the chiral magnet's and baby Skyrme's initialize(mode="initial") cannot run in the
+ * reference (one argument short). */
+int ss_initialize(ss_handle *h, void *field, void *velocity, int mode, int ansatz, double rotation,
+                  double vortex_number);
+/* Add one soliton centred on lattice point (pxi, pxj) to the field in place:
+ * chiral magnet / baby Skyrme: the `ansatz` skyrmion composed stereographically with
+ * the field there (create_skyrmion_kernel, chiral_magnet/initial_config.py:285-386);
+ * Abelian Higgs / s+id: a vortex (`vortex` != 0: phase -theta, else +theta) multiplied
+ * into the condensates (create_vortex_kernel, ginzburg_landau_superconductor/
+ * initial_config.py:259-313, anisotropic_superconductor/initial_config.py:282-347).
+ * A point outside the lattice leaves the field unchanged, as in the reference. */
+int ss_insert_soliton(ss_handle *h, void *field, int pxi, int pxj, int ansatz, int vortex, double rotation);
+
+/* Headless RGBA image of a lattice into a caller-owned device buffer of ylen*xlen*4
+ * bytes (4-byte aligned; pixel (y, x) at byte 4*(y*xlen + x), R G B A), the bytes
+ * the reference's viewer writes into its GL pixel buffer, without a graphics context.
+ * SS_RENDER_JET / SS_RENDER_GRAY: src is a density indexed y + x*ylen, normalised by
+ * vmin/vmax; SS_RENDER_MAGNETIZATION: src holds the planes m1, m2, m3 (stride
+ * xlen*ylen; vmin/vmax unused).  precision (SS_FP32 or SS_FP64) is src's element
+ * type; the arithmetic is FP64.  Asynchronous on `stream`.  Replaces
+ * render_jet_density_to_rgba, render_gray_density_to_rgba and
+ * render_magnetization_to_rgba (soliton_solver/core/colormaps.py:94-267). */
+int ss_render_rgba(int kind, const void *src, int precision, int xlen, int ylen, double vmin, double vmax,
+                   unsigned char *rgba, void *stream);
 /* Charge densities / totals.  Replace compute_skyrmion_number_kernel,
  * compute_magnetic_charge_kernel, compute_vortex_number_kernel and the matching
  * observables.compute_* (e.g. theories/chiral_magnet/kernels.py:294-395,

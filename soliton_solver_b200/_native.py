@@ -37,6 +37,19 @@ SS_CHARGE_SKYRMION = 0
 SS_CHARGE_MAGNETIC = 1
 SS_CHARGE_VORTEX = 2
 
+# initial conditions (ss_initialize, ss_insert_soliton)
+SS_INIT_GROUND = 0
+SS_INIT_ANSATZ = 1
+SS_ANSATZ_NONE = 0
+SS_ANSATZ_BLOCH = 1
+SS_ANSATZ_NEEL = 2
+SS_ANSATZ_ANTI = 3
+
+# colormaps (ss_render_rgba)
+SS_RENDER_JET = 0
+SS_RENDER_GRAY = 1
+SS_RENDER_MAGNETIZATION = 2
+
 # couplings
 SS_COUPLING_KAPPA = 0
 SS_COUPLING_MPI = 1
@@ -88,6 +101,9 @@ _SIG = {
     "ss_energy_density": ([_P, _P, _P], _I),
     "ss_energy": ([_P, _P, ctypes.POINTER(_D)], _I),
     "ss_energy_projected": ([_P, _P, ctypes.POINTER(_D)], _I),
+    "ss_render_rgba": ([_I, _P, _I, _I, _I, _D, _D, _P, _P], _I),
+    "ss_initialize": ([_P, _P, _P, _I, _I, _D, _D], _I),
+    "ss_insert_soliton": ([_P, _P, _I, _I, _I, _I, _D], _I),
     "ss_charge_density": ([_P, _P, _I, _P], _I),
     "ss_charge": ([_P, _P, _I, ctypes.POINTER(_D)], _I),
     "ss_coupling_grad": ([_P, _P, _I, ctypes.POINTER(_D)], _I),

@@ -146,6 +146,26 @@ class Solver:
         return {m: (float(ms[2 * m]), float(ms[2 * m + 1]), int(self._lib.ss_get_variant(self._h, m)))
                 for m in (1, 2, 3, 4)}
 
+    def initialize(self, field, velocity=None, mode: int = nat.SS_INIT_GROUND, ansatz: int = nat.SS_ANSATZ_BLOCH,
+                   rotation: float = 0.0, vortex_number: float = 1.0):
+        """Ground state or single-soliton ansatz into `field` (velocity zeroed if given);
+        see ss_initialize.  Asynchronous on the solver's stream."""
+        self._check(field)
+        if velocity is not None:
+            self._check(velocity)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_initialize(self._h, _ptr(field), _ptr(velocity), int(mode), int(ansatz),
+                                              float(rotation), float(vortex_number)))
+
+    def insert_soliton(self, field, pxi: int, pxj: int, ansatz: int = nat.SS_ANSATZ_BLOCH, vortex: int = 1,
+                       rotation: float = 0.0):
+        """Add a skyrmion (chiral magnet, baby Skyrme) or a vortex (Abelian Higgs, s+id)
+        centred on lattice point (pxi, pxj) to `field`; see ss_insert_soliton."""
+        self._check(field)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_insert_soliton(self._h, _ptr(field), int(pxi), int(pxj), int(ansatz),
+                                                  int(vortex), float(rotation)))
+
     def set_variant(self, stage: int, variant: int):
         """Pin the staging variant of flow mode `stage` (0 gradient, 1-4 stages):
         0 one tile per CTA, 1 pipelined (see ss_set_variant)."""

@@ -15,6 +15,8 @@
 #include "flow.cuh"
 #include "plain.cuh"
 #include "batch.cuh"
+#include "render.cuh"
+#include "init.cuh"
 #include "theories.cuh"
 
 using namespace ssb;
@@ -79,6 +81,7 @@ bool encode_tile_map(CUtensorMap* m, const void* ptr, size_t es, int X, int Y, i
 
 struct ss_handle {
   int theory = 0, precision = 0, nf = 0;
+  double pf_raw[32] = {};  // the packed p_f as given (initial-condition kernels read it)
   Grid G{};
   Phys P{};
   size_t elem = 8;
@@ -172,6 +175,7 @@ int decode(ss_handle* h, int theory, const int32_t* p_i, int n_i, const double* 
   if (n_i < need_i[theory] || n_f < need_f[theory])
     return fail(SS_ERR_ARG, "packed params too short for theory %d: n_i=%d (need %d), n_f=%d (need %d)", theory, n_i,
                 need_i[theory], n_f, need_f[theory]);
+  for (int i = 0; i < n_f && i < 32; ++i) h->pf_raw[i] = p_f[i];
   Grid& G = h->G;
   G.X = p_i[0];
   G.Y = p_i[1];
@@ -1018,6 +1022,87 @@ int ss_energy(ss_handle* h, const void* field, double* out) {
   });
   if (rc) return rc;
   return scalar_result(h, out);
+}
+
+namespace {
+int launch_init(ss_handle* h, void* field, void* velocity, const InitArgs& A) {
+  const long long N = (long long)A.X * A.Y;
+  const unsigned blocks = (unsigned)((N + 255) / 256);
+  auto go = [&](auto* tag) -> int {
+    using R = std::remove_pointer_t<decltype(tag)>;
+    R* F = (R*)field;
+    R* V = (R*)velocity;
+    switch (h->theory) {
+      case 0: init_kernel<0, R><<<blocks, 256, 0, h->stream>>>(F, V, A); break;
+      case 1: init_kernel<1, R><<<blocks, 256, 0, h->stream>>>(F, V, A); break;
+      case 2: init_kernel<2, R><<<blocks, 256, 0, h->stream>>>(F, V, A); break;
+      default: init_kernel<3, R><<<blocks, 256, 0, h->stream>>>(F, V, A); break;
+    }
+    CK(cudaGetLastError());
+    return SS_OK;
+  };
+  return h->precision == SS_FP32 ? go((float*)nullptr) : go((double*)nullptr);
+}
+
+InitArgs init_args(const ss_handle* h, int mode) {
+  InitArgs A;
+  memset(&A, 0, sizeof(A));
+  A.X = h->G.X;
+  A.Y = h->G.Y;
+  A.nf = h->nf;
+  A.mode = mode;
+  for (int i = 0; i < 32; ++i) A.pf[i] = h->pf_raw[i];
+  return A;
+}
+}  // namespace
+
+int ss_initialize(ss_handle* h, void* field, void* velocity, int mode, int ansatz, double rotation,
+                  double vortex_number) {
+  if (!h || !field) return fail(SS_ERR_ARG, "handle and field must not be NULL");
+  if (mode != SS_INIT_GROUND && mode != SS_INIT_ANSATZ) return fail(SS_ERR_ARG, "unknown init mode %d", mode);
+  if (ansatz < SS_ANSATZ_NONE || ansatz > SS_ANSATZ_ANTI) return fail(SS_ERR_ARG, "unknown ansatz %d", ansatz);
+  InitArgs A = init_args(h, mode == SS_INIT_GROUND ? IM_GROUND : IM_ANSATZ);
+  A.ansatz = ansatz;
+  A.rotation = rotation;
+  A.vortex_number = vortex_number;
+  return launch_init(h, field, velocity, A);
+}
+
+int ss_insert_soliton(ss_handle* h, void* field, int pxi, int pxj, int ansatz, int vortex, double rotation) {
+  if (!h || !field) return fail(SS_ERR_ARG, "handle and field must not be NULL");
+  if (ansatz < SS_ANSATZ_NONE || ansatz > SS_ANSATZ_ANTI) return fail(SS_ERR_ARG, "unknown ansatz %d", ansatz);
+  if (pxi < 0 || pxi >= h->G.X || pxj < 0 || pxj >= h->G.Y) return SS_OK;  // the reference's kernels ignore it
+  InitArgs A = init_args(h, IM_INSERT);
+  A.ansatz = ansatz;
+  A.vortex = vortex ? 1 : 0;
+  A.rotation = rotation;
+  A.pxi = pxi;
+  A.pxj = pxj;
+  return launch_init(h, field, nullptr, A);
+}
+
+int ss_render_rgba(int kind, const void* src, int precision, int xlen, int ylen, double vmin, double vmax,
+                   unsigned char* rgba, void* stream) {
+  if (!src || !rgba) return fail(SS_ERR_ARG, "src and rgba must not be NULL");
+  if (kind < SS_RENDER_JET || kind > SS_RENDER_MAGNETIZATION) return fail(SS_ERR_ARG, "unknown render kind %d", kind);
+  if (precision != SS_FP32 && precision != SS_FP64)
+    return fail(SS_ERR_ARG, "precision must be SS_FP32 or SS_FP64 (element type of src)");
+  if (xlen <= 0 || ylen <= 0) return fail(SS_ERR_ARG, "xlen and ylen must be positive");
+  if ((reinterpret_cast<uintptr_t>(rgba) & 3u) != 0) return fail(SS_ERR_ARG, "rgba must be 4-byte aligned");
+  const dim3 grid((unsigned)((ylen + 31) / 32), (unsigned)((xlen + 31) / 32)), block(32, 8);
+  if (grid.y > 65535u) return fail(SS_ERR_ARG, "xlen %d too large (at most %d)", xlen, 65535 * 32);
+  cudaStream_t s = (cudaStream_t)stream;
+  uint32_t* out = reinterpret_cast<uint32_t*>(rgba);
+  auto go = [&](auto* tag) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    const T* p = (const T*)src;
+    if (kind == SS_RENDER_JET) render_kernel<T, RK_JET><<<grid, block, 0, s>>>(p, xlen, ylen, vmin, vmax, out);
+    else if (kind == SS_RENDER_GRAY) render_kernel<T, RK_GRAY><<<grid, block, 0, s>>>(p, xlen, ylen, vmin, vmax, out);
+    else render_kernel<T, RK_MAGNETIZATION><<<grid, block, 0, s>>>(p, xlen, ylen, vmin, vmax, out);
+  };
+  if (precision == SS_FP32) go((float*)nullptr); else go((double*)nullptr);
+  CK(cudaGetLastError());
+  return SS_OK;
 }
 
 int ss_energy_projected(ss_handle* h, const void* field, double* out) {

@@ -85,3 +85,16 @@ def test_short_param_arrays_and_bad_ids():
     assert lib.ss_create(0, p_i.ctypes.data, 4, p_f.ctypes.data, 4, 1, ctypes.byref(h)) == nat.SS_ERR_ARG
     assert lib.ss_create(9, p_i.ctypes.data, 4, p_f.ctypes.data, 4, 1, ctypes.byref(h)) == nat.SS_ERR_ARG
     assert lib.ss_create(0, p_i.ctypes.data, 4, p_f.ctypes.data, 4, 7, ctypes.byref(h)) == nat.SS_ERR_ARG
+
+
+def test_render_rgba_validates_arguments_on_the_host():
+    """ss_render_rgba rejects bad arguments before launching anything."""
+    lib = nat.load()
+    buf = ctypes.c_void_p(64)  # never dereferenced: every call below fails validation first
+    assert lib.ss_render_rgba(nat.SS_RENDER_JET, None, nat.SS_FP64, 4, 4, 0.0, 1.0, buf, None) == nat.SS_ERR_ARG
+    assert lib.ss_render_rgba(7, buf, nat.SS_FP64, 4, 4, 0.0, 1.0, buf, None) == nat.SS_ERR_ARG
+    assert lib.ss_render_rgba(nat.SS_RENDER_GRAY, buf, nat.SS_PLAIN_FP64, 4, 4, 0.0, 1.0, buf, None) == nat.SS_ERR_ARG
+    assert lib.ss_render_rgba(nat.SS_RENDER_GRAY, buf, nat.SS_FP32, 0, 4, 0.0, 1.0, buf, None) == nat.SS_ERR_ARG
+    assert lib.ss_render_rgba(nat.SS_RENDER_GRAY, buf, nat.SS_FP32, 4, 4, 0.0, 1.0, ctypes.c_void_p(66), None) \
+        == nat.SS_ERR_ARG
+    assert b"aligned" in lib.ss_last_error()
