@@ -484,6 +484,46 @@ def initial_condition(dev, reps=10):
             "us": us, "achieved_gbs": XLEN * YLEN * 32 / (us * 1e-6) / 1e9, "bytes_per_site": 32}
 
 
+def dat_field_dump(dev, F0, reps=3):
+    """The .dat text of the workload's 4096^2 x 4 FP32 field at 32 significant digits
+    (output_field_dat's bytes) formatted on the GPU (ss_format_text: length pass, scan,
+    write pass), device-resident text; against the reference writer's per-value Python
+    formatting timed on a 200 000-value sample of the same field."""
+    import ctypes
+    import torch
+    from soliton_solver_b200 import _native as nat
+    from oracle import io as oio
+    v = F0.to(device=dev, dtype=torch.float32).contiguous().reshape(-1)
+    n = v.numel()
+    lib = nat.load()
+    nb = ctypes.c_size_t()
+    nat.check(lib.ss_text_workspace_bytes(n, ctypes.byref(nb)))
+    ws = torch.empty(int(nb.value), dtype=torch.uint8, device=dev)
+    length = ctypes.c_longlong()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    args = (v.data_ptr(), nat.SS_FP32, n, 32, YLEN, XLEN * YLEN)
+    nat.check(lib.ss_format_text(*args, None, 0, ctypes.byref(length), ws.data_ptr(), ws.numel(), stream))
+    out = torch.empty(int(length.value), dtype=torch.uint8, device=dev)
+    ts = []
+    for _ in range(reps):
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter()
+        nat.check(lib.ss_format_text(*args, out.data_ptr(), out.numel(), ctypes.byref(length), ws.data_ptr(),
+                                     ws.numel(), stream))
+        torch.cuda.synchronize(dev)
+        ts.append(time.perf_counter() - t)
+    dt = min(ts)
+    sample = v[:200000].cpu().numpy()
+    t = time.perf_counter()
+    oio.field_text(sample, 1, 200000, 1, 32)
+    py = 200000 / (time.perf_counter() - t)
+    del out, ws
+    torch.cuda.empty_cache()
+    return {"values": n, "text_bytes": int(length.value), "s": dt, "values_per_s": n / dt,
+            "text_gbs": length.value / dt / 1e9, "python_format_values_per_s": py, "speedup": n / dt / py,
+            "note": "ss_format_text incl. its length pass, scan and one stream sync; wall clock"}
+
+
 def compare_fp64_and_plain(args, dev, F0):
     """Relaxed-state accuracy (320^2), and the plain-FP64 form's speed on this lattice."""
     import torch
@@ -492,7 +532,7 @@ def compare_fp64_and_plain(args, dev, F0):
     out = {}
     for key, fn in (("accuracy", relaxed_accuracy), ("batched_sweep", batched_sweep),
                     ("graph_320", small_lattice_graph), ("render_rgba", lambda d: render_rgba(d, F0)),
-                    ("initial_condition", initial_condition)):
+                    ("initial_condition", initial_condition), ("dat_field_dump", lambda d: dat_field_dump(d, F0))):
         try:
             out[key] = fn(dev)
         except Exception as exc:  # reported, not fatal: the headline line must still print

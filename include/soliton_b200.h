@@ -194,6 +194,23 @@ int ss_initialize(ss_handle *h, void *field, void *velocity, int mode, int ansat
  * A point outside the lattice leaves the field unchanged, as in the reference. */
 int ss_insert_soliton(ss_handle *h, void *field, int pxi, int pxj, int ansatz, int vortex, double rotation);
 
+/* Plain-text formatting of n values on the device, byte for byte as the reference's
+ * .dat writers (core/io.py:44-240): each value as Python's format(v, ".{digits}g")
+ * (exact decimal conversion, round half to even, "g" presentation, "nan", "inf",
+ * "-0"), followed by a tab; a newline after every `row` values and another after
+ * every `block` values (0: none).  output_field_dat is row = ylen, block = xlen*ylen;
+ * output_density_data_dat row = ylen, block = 0; output_iteration_data_dat row =
+ * block = 0.  values: device array of SS_FP32 or SS_FP64 (`precision`); digits 1..40.
+ * workspace: device scratch of ss_text_workspace_bytes(n) bytes, 8-byte aligned.  With
+ * out == NULL only *out_len (the text's length) is computed; otherwise the text is
+ * written to the device buffer out (out_cap bytes) and *out_len set.  Synchronises
+ * the stream once (to read the length).  Replaces output_field_dat,
+ * output_density_data_dat and output_iteration_data_dat's formatting loops. */
+int ss_text_workspace_bytes(long long n, size_t *bytes);
+int ss_format_text(const void *values, int precision, long long n, int digits, long long row, long long block,
+                   char *out, size_t out_cap, long long *out_len, void *workspace, size_t workspace_bytes,
+                   void *stream);
+
 /* Headless RGBA image of a lattice into a caller-owned device buffer of ylen*xlen*4
  * bytes (4-byte aligned; pixel (y, x) at byte 4*(y*xlen + x), R G B A), the bytes
  * the reference's viewer writes into its GL pixel buffer, without a graphics context.

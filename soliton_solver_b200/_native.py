@@ -103,6 +103,9 @@ _SIG = {
     "ss_energy_projected": ([_P, _P, ctypes.POINTER(_D)], _I),
     "ss_render_rgba": ([_I, _P, _I, _I, _I, _D, _D, _P, _P], _I),
     "ss_initialize": ([_P, _P, _P, _I, _I, _D, _D], _I),
+    "ss_text_workspace_bytes": ([ctypes.c_longlong, ctypes.POINTER(ctypes.c_size_t)], _I),
+    "ss_format_text": ([_P, _I, ctypes.c_longlong, _I, ctypes.c_longlong, ctypes.c_longlong, _P, ctypes.c_size_t,
+                        ctypes.POINTER(ctypes.c_longlong), _P, ctypes.c_size_t, _P], _I),
     "ss_insert_soliton": ([_P, _P, _I, _I, _I, _I, _D], _I),
     "ss_charge_density": ([_P, _P, _I, _P], _I),
     "ss_charge": ([_P, _P, _I, ctypes.POINTER(_D)], _I),

@@ -126,6 +126,34 @@ class Simulation:
         without a unit-vector constraint."""
         return self.solver.energy_projected(self.Field)
 
+    def save_output(self, output_dir: str | None = None, precision: int = 32):
+        """The theory's .dat output bundle (soliton_solver/core/simulation.py save_output):
+        lattice sizes and vectors, the field dump and the component grids of the field,
+        the energy density and the theory's charge densities, formatted on the GPU.
+        Arrays this backend does not compute (supercurrent, magnetic flux density) are
+        passed as None and their files skipped, as the reference skips missing arrays.
+        The default directory is the theory package's ``results``."""
+        import inspect
+        import os
+        if output_dir is None:
+            output_dir = os.path.join(os.path.dirname(os.path.abspath(self.theory.io.__file__)), "results")
+        os.makedirs(output_dir, exist_ok=True)
+        self.kernels.create_grid_kernel[None, None](self.grid, self.p_i_h, self.p_f_h)
+        om = self.observables_mod
+        dens = {"h_EnergyDensity": self.solver.energy_density(self.Field).clone()}
+        if hasattr(om, "compute_skyrmion_number"):
+            dens["h_BaryonDensity"] = self.solver.charge_density(self.Field, "skyrmion").clone()
+        if hasattr(om, "compute_magnetic_charge"):
+            dens["h_MagneticChargeDensity"] = self.solver.charge_density(self.Field, "magnetic").clone()
+        if hasattr(om, "compute_vortex_number"):
+            dens["h_VortexDensity"] = self.solver.charge_density(self.Field, "vortex").clone()
+        kwargs = dict(output_dir=output_dir, h_Field=self.Field, h_grid=self.grid, h_Supercurrent=None,
+                      h_MagneticFluxDensity=None, xlen=int(self.p_i_h[0]), ylen=int(self.p_i_h[1]),
+                      number_coordinates=int(self.p_i_h[3]), number_total_fields=int(self.p_i_h[4]),
+                      precision=precision, **dens)
+        accepted = set(inspect.signature(self.theory.io.output_data_bundle).parameters)
+        self.theory.io.output_data_bundle(**{k: v for k, v in kwargs.items() if k in accepted})
+
     def compute_energy_density(self):
         self.solver.energy_density(self.Field, self.en)
         torch.cuda.synchronize(self.device)

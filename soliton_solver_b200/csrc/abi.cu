@@ -17,6 +17,7 @@
 #include "batch.cuh"
 #include "render.cuh"
 #include "init.cuh"
+#include "text.cuh"
 #include "theories.cuh"
 
 using namespace ssb;
@@ -1079,6 +1080,50 @@ int ss_insert_soliton(ss_handle* h, void* field, int pxi, int pxj, int ansatz, i
   A.pxi = pxi;
   A.pxj = pxj;
   return launch_init(h, field, nullptr, A);
+}
+
+int ss_text_workspace_bytes(long long n, size_t* bytes) {
+  if (!bytes || n < 0) return fail(SS_ERR_ARG, "bad arguments");
+  const long long nb = (n + 1023) / 1024;
+  *bytes = (size_t)(n + nb + 8) * sizeof(long long);
+  return SS_OK;
+}
+
+int ss_format_text(const void* values, int precision, long long n, int digits, long long row, long long block,
+                   char* out, size_t out_cap, long long* out_len, void* workspace, size_t workspace_bytes,
+                   void* stream) {
+  if (!values || !out_len || !workspace) return fail(SS_ERR_ARG, "values, out_len and workspace must not be NULL");
+  if (precision != SS_FP32 && precision != SS_FP64) return fail(SS_ERR_ARG, "precision must be SS_FP32 or SS_FP64");
+  if (n <= 0) return fail(SS_ERR_ARG, "n must be positive");
+  if (digits < 1 || digits > TXT_MAX_P) return fail(SS_ERR_ARG, "digits must be 1..%d", TXT_MAX_P);
+  if (row < 0 || block < 0) return fail(SS_ERR_ARG, "row and block must be >= 0");
+  size_t need = 0;
+  ss_text_workspace_bytes(n, &need);
+  if (workspace_bytes < need) return fail(SS_ERR_WORKSPACE, "workspace of %zu bytes, need %zu", workspace_bytes, need);
+  if ((reinterpret_cast<uintptr_t>(workspace) & 7u) != 0) return fail(SS_ERR_WORKSPACE, "workspace must be 8-byte aligned");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long nb = (n + 1023) / 1024;
+  long long* off = (long long*)workspace;
+  long long* sums = off + n;
+  long long* total = sums + nb;
+  const TextLayout L{n, row, block, digits};
+  const unsigned g256 = (unsigned)((n + 255) / 256);
+  if (precision == SS_FP32) text_len_kernel<float><<<g256, 256, 0, st>>>((const float*)values, L, off);
+  else text_len_kernel<double><<<g256, 256, 0, st>>>((const double*)values, L, off);
+  scan_block_kernel<<<(unsigned)nb, 1024, 0, st>>>(off, n, sums);
+  scan_sums_kernel<<<1, 1024, 0, st>>>(sums, nb, total);
+  scan_add_kernel<<<(unsigned)nb, 1024, 0, st>>>(off, n, sums);
+  CK(cudaGetLastError());
+  long long len = 0;
+  CK(cudaMemcpyAsync(&len, total, sizeof(len), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  *out_len = len;
+  if (!out) return SS_OK;  // size query
+  if ((size_t)len > out_cap) return fail(SS_ERR_ARG, "text of %lld bytes does not fit the %zu-byte buffer", len, out_cap);
+  if (precision == SS_FP32) text_write_kernel<float><<<g256, 256, 0, st>>>((const float*)values, L, off, out);
+  else text_write_kernel<double><<<g256, 256, 0, st>>>((const double*)values, L, off, out);
+  CK(cudaGetLastError());
+  return SS_OK;
 }
 
 int ss_render_rgba(int kind, const void* src, int precision, int xlen, int ylen, double vmin, double vmax,

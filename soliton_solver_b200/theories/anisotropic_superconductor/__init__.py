@@ -8,6 +8,7 @@ from . import params
 from . import kernels
 from . import initial_config
 from . import observables
+from . import io
 
 THEORY_SPEC = TheorySpec(
     name='Anisotropic superconductor',
