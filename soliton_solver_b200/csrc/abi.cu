@@ -343,13 +343,13 @@ struct Fused {
     return fail(SS_ERR_ARG, "bad flow mode");
   }
 
-  // persistent TMA-pipelined variant: FP32 fields and at least two ring slots
-  static constexpr int PIPE_NT = 512;
+  // persistent TMA-pipelined variant: FP32 fields and at least two ring slots; threads
+  // and resident CTAs per SM from pipe_threads / pipe_ctas
   template <int MODE>
   static constexpr int pipe_stages() {
     const size_t slot = pipe_slot_bytes<R, TH::NF, TX, TY, MODE>();
     // dynamic shared memory left next to the static reduction arrays, per resident CTA
-    const size_t budget = pipe_ctas<TH, MODE>() == 2 ? 100 * 1024 : 212 * 1024;
+    const size_t budget = pipe_ctas<TH, MODE>() == 4 ? 50 * 1024 : 212 * 1024;
     const int n = (int)(budget / slot);
     return n > 4 ? 4 : n;
   }
@@ -363,11 +363,12 @@ struct Fused {
   static int launch_pipe(const ss_handle* h, const FlowArgs<R>& A) {
     if constexpr (pipe_ok<MODE>()) {
       constexpr int S = pipe_stages<MODE>();
-      auto k = flow_kernel_pipe<TH, R, TX, TY, PIPE_NT, MODE, S>;
+      constexpr int NTP = pipe_threads<TH, MODE>();
+      auto k = flow_kernel_pipe<TH, R, TX, TY, NTP, MODE, S>;
       const size_t smem = S * pipe_slot_bytes<R, TH::NF, TX, TY, MODE>();
       set_smem(k, smem, smem_done_pipe[MODE]);
       const int grid = std::min(h->nblocks, pipe_ctas<TH, MODE>() * h->num_sms);
-      k<<<grid, PIPE_NT, smem, h->stream>>>(A);
+      k<<<grid, NTP, smem, h->stream>>>(A);
       CK(cudaGetLastError());
       return SS_OK;
     } else {

@@ -730,12 +730,18 @@ __host__ __device__ constexpr size_t pipe_slot_bytes() {
          sizeof(R) * NF * TX * TY * pipe_centre_buffers<MODE>();
 }
 
-// Persistent CTAs per SM: two for stage 1 and the energy pass of a theory whose
-// energy point runs in packed FP32 (latency-bound, so twice the warps help), one
-// otherwise.  Stage 1 and the energy pass must agree: their partials are per CTA.
+// Persistent CTAs per SM: four 256-thread CTAs for stage 1 and the energy pass of a
+// theory whose energy point runs in packed FP32 (issue-bound: two site pairs per thread
+// per tile halve the per-tile overhead, and four CTAs keep 32 warps per SM), one
+// 512-thread CTA otherwise.  Stage 1 and the energy pass must agree: their partials
+// are per CTA.
 template <class TH, int MODE>
 __host__ __device__ constexpr int pipe_ctas() {
-  return ((MODE == M_S1 || MODE == M_ENERGY) && TH::PAIR_ENERGY) ? 2 : 1;
+  return ((MODE == M_S1 || MODE == M_ENERGY) && TH::PAIR_ENERGY) ? 4 : 1;
+}
+template <class TH, int MODE>
+__host__ __device__ constexpr int pipe_threads() {
+  return pipe_ctas<TH, MODE>() == 4 ? 256 : 512;
 }
 
 template <class TH, typename R, int TX, int TY, int NT, int MODE, int STAGES>
