@@ -33,7 +33,9 @@ XLEN = YLEN = 4096
 XSIZE = 128.0
 METRIC = "Mpoint-updates/s per flow step at dE/E<=1e-6 vs plain FP64; achieved HBM GB/s"
 UNIT = "Mpoint-updates/s"
-WORDS_PER_SITE_STEP = 16  # S1: 2, S2: 3, S3: 4, S4: 7 words of nf components
+# words of nf components moved per site and step: S1 2, S2 3, S3 4, S4 7 as four
+# kernels; S1 2, S2+S3 fused 5, S4 7 when stages 2 and 3 run as one kernel
+WORDS_SEPARATE, WORDS_FUSED = 16, 14
 
 
 def chiral_params(xlen=None, ylen=None, xsize=None):
@@ -229,7 +231,7 @@ def gpu_arm(args, rank, world, local_rank):
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     ms_step = ms / K
     value = world * N * K / (ms / 1e3) / 1e6
-    launches = 4 * K + 2
+    launches = (3 if (s.tma_enabled and s._lib.ss_get_variant(s._h, 6) == 1) else 4) * K + 2
 
     # roofline of the fused stage kernel (4 launches per step)
     from soliton_solver_b200._native import load as _load  # noqa: F401 (library loaded)
@@ -240,7 +242,9 @@ def gpu_arm(args, rank, world, local_rank):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    bytes_step = WORDS_PER_SITE_STEP * 4 * 4 * N
+    fused = s.tma_enabled and s._lib.ss_get_variant(s._h, 6) == 1
+    words = WORDS_FUSED if fused else WORDS_SEPARATE
+    bytes_step = words * 4 * 4 * N
     achieved = bytes_step / (ms_step / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "flow_kernel_traffic.json")
@@ -286,14 +290,18 @@ def gpu_arm(args, rank, world, local_rank):
                                   "global_sites": world * N}),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                             "kernel": "flow_kernel<ChiralMagnet,float> (4 stage launches per step)",
+                             "kernel": "flow_kernel<ChiralMagnet,float> stage launches (S1, S2+S3 fused, S4)"
+                                       if fused else "flow_kernel<ChiralMagnet,float> (4 stage launches per step)",
+                             "launches_per_step": 3 if fused else 4,
                              "algorithmic_bytes_per_step": bytes_step},
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": Ke, "api": "Simulation.step(prev_energy) per step"},
                 "gpu_launches": launches, "clocks": clk.summary(),
-                "autotune": {f"S{m}": {"tile_per_cta_ms": a, "pipelined_ms": b, "chosen": "pipelined" if c else
-                                       "tile_per_cta"} for m, (a, b, c) in tuning.items()}}
+                "autotune": {**{f"S{m}": {"tile_per_cta_ms": a, "pipelined_ms": b, "chosen": "pipelined" if c else
+                                          "tile_per_cta"} for m, (a, b, c) in tuning.items() if m != 6},
+                             "S2+S3": {"two_kernels_ms": tuning[6][0], "fused_ms": tuning[6][1],
+                                       "chosen": "fused" if tuning[6][2] else "two kernels"}}}
         line.update(extra)
         print(json.dumps(line), flush=True)
     return 0

@@ -123,17 +123,21 @@ int ss_check_status(ss_handle *h);
  * (row pitch and base 16-byte aligned), 0 when the plain-load path is used. */
 int ss_tma_enabled(const ss_handle *h);
 /* Autotuner: times, on the bound buffers, the two TMA staging variants of each flow
- * stage (a persistent CTA per SM walking tiles through a shared-memory ring, or one
- * tile per CTA) over `iters` launches and keeps the faster one.  Writes only
- * workspace scratch.  ms_out (nullable, 12 floats) receives [mode][variant] times. */
+ * stage (persistent CTAs walking tiles through a shared-memory ring, or one tile per
+ * CTA) over `iters` launches and keeps the faster one, then times stages 2 and 3 fused
+ * into one kernel (one staging of phi, V, l1) against the two chosen kernels.  Writes
+ * only workspace scratch.  ms_out (nullable, 14 floats) receives [mode][variant]
+ * times for modes 0..6 (mode 6: [two kernels, fused]). */
 int ss_autotune(ss_handle *h, int iters, float *ms_out);
-/* Variant chosen for a flow mode (0..5): 1 pipelined, 0 one tile per CTA, -1 bad args. */
+/* Variant chosen for a flow mode (0..5): 1 pipelined, 0 one tile per CTA; mode 6: 1 if
+ * stages 2 and 3 run fused; -1 bad args. */
 int ss_get_variant(const ss_handle *h, int mode);
 /* Pin the staging variant of a flow mode instead of autotuning it: mode 0 (gradient)
  * or 1..4 (stages; stage 1 also sets the energy pass, whose per-CTA partials must
  * match it), variant 0 (one tile per CTA) or 1 (pipelined; needs TMA-staged bound
- * buffers and FP32 fields).  For reproducible runs and for profiling a known kernel
- * set.  No reference counterpart (tuning control). */
+ * buffers and FP32 fields); mode 6: 1 runs stages 2 and 3 as one kernel (with TMA
+ * staging), 0 as two.  For reproducible runs and for profiling a known kernel set.
+ * No reference counterpart (tuning control). */
 int ss_set_variant(ss_handle *h, int mode, int variant);
 /* Failure-detection hook.  Sets the bound (clock64 cycles, default 2e9) of every
  * device-side mbarrier wait of this handle's kernels; with inject != 0 the next

@@ -139,12 +139,13 @@ class Solver:
     def autotune(self, iters: int = 5):
         """Pick the faster TMA staging variant of each flow stage on the bound buffers.
 
-        Returns {stage: (ms one-tile-per-CTA, ms pipelined, chosen)} for stages 1-4."""
-        ms = np.zeros(12, dtype=np.float32)
+        Returns {stage: (ms one-tile-per-CTA, ms pipelined, chosen)} for stages 1-4 and
+        {6: (ms stages 2 and 3 as two kernels, ms fused, 1 if fused)}."""
+        ms = np.zeros(14, dtype=np.float32)
         with torch.cuda.device(self.device):
             nat.check(self._lib.ss_autotune(self._h, int(iters), ms.ctypes.data))
         return {m: (float(ms[2 * m]), float(ms[2 * m + 1]), int(self._lib.ss_get_variant(self._h, m)))
-                for m in (1, 2, 3, 4)}
+                for m in (1, 2, 3, 4, 6)}
 
     def initialize(self, field, velocity=None, mode: int = nat.SS_INIT_GROUND, ansatz: int = nat.SS_ANSATZ_BLOCH,
                    rotation: float = 0.0, vortex_number: float = 1.0):

@@ -118,8 +118,9 @@ struct ss_handle {
   bool tma = false;
   int num_sms = 148;
   // per flow mode: 1 = persistent pipelined kernel, 0 = one tile per CTA (autotuned)
-  int use_pipe[6] = {1, 1, 1, 1, 1, 1};
-  float tune_ms[6][2] = {};
+  int use_pipe[N_FLOW_MODES] = {1, 1, 1, 1, 1, 1, 0};
+  float tune_ms[N_FLOW_MODES][2] = {};
+  int fuse23 = 1;  // stages 2 and 3 in one kernel (TMA staging only)
   long long wait_cycles = WAIT_CYCLES;
   mutable int inject_timeout = 0;  // test hook, consumed by the next flow launch
   cudaGraphExec_t graph = nullptr;  // captured n-step relaxation (ss_graph_create)
@@ -312,7 +313,7 @@ struct Fused {
   static inline unsigned long long smem_done_density = 0;
 
   // tma: use the TMA-staged instantiation (A.tm_* must describe A's buffers)
-  static inline unsigned long long smem_done[2][6] = {};
+  static inline unsigned long long smem_done[2][N_FLOW_MODES] = {};
 
   // dynamic shared memory of flow_kernel: the staged buffers
   template <bool TMA_, int MODE>
@@ -339,6 +340,9 @@ struct Fused {
       case M_S3: return launch_mode<TMA_, M_S3>(h, A);
       case M_S4: return launch_mode<TMA_, M_S4>(h, A);
       case M_ENERGY: return launch_mode<TMA_, M_ENERGY>(h, A);
+      case M_S23:
+        if constexpr (TMA_) return launch_mode<TMA_, M_S23>(h, A);
+        else return fail(SS_ERR_ARG, "the fused stages 2+3 need TMA staging");
     }
     return fail(SS_ERR_ARG, "bad flow mode");
   }
@@ -357,7 +361,7 @@ struct Fused {
   static constexpr bool pipe_ok() {
     return sizeof(R) == 4 && pipe_stages<MODE>() >= 2;
   }
-  static inline unsigned long long smem_done_pipe[6] = {};
+  static inline unsigned long long smem_done_pipe[N_FLOW_MODES] = {};
 
   template <int MODE>
   static int launch_pipe(const ss_handle* h, const FlowArgs<R>& A) {
@@ -461,15 +465,26 @@ struct Fused {
       A.arrest_update = 0;
       A.init_state = 0;
       A.E_idx = -1;
-      // S2, S3
-      A.mode = M_S2;
-      A.out_l = l2;
-      if ((rc = launch(h, A, tma))) return rc;
-      A.mode = M_S3;
-      A.la = l1;
-      A.out_l = l3;
-      if (tma) A.tm_l = h->tm[4];
-      if ((rc = launch(h, A, tma))) return rc;
+      // S2, S3: one fused kernel on TMA-staged buffers (one staging of phi, V, l1),
+      // else two
+      if (tma && h->fuse23) {
+        A.mode = M_S23;
+        A.la = l1;
+        A.out_l = l3;
+        A.out_l2 = l2;
+        A.tm_l = h->tm[4];
+        if ((rc = launch(h, A, tma))) return rc;
+        A.out_l2 = nullptr;
+      } else {
+        A.mode = M_S2;
+        A.out_l = l2;
+        if ((rc = launch(h, A, tma))) return rc;
+        A.mode = M_S3;
+        A.la = l1;
+        A.out_l = l3;
+        if (tma) A.tm_l = h->tm[4];
+        if ((rc = launch(h, A, tma))) return rc;
+      }
       // S4 + finalize into the ping-pong buffers
       A.mode = M_S4;
       A.la = l1;
@@ -554,6 +569,26 @@ struct Fused {
     // the energy-only pass must reduce exactly like stage 1 (same grid and tile order)
     h->use_pipe[M_ENERGY] = h->use_pipe[M_S1];
     h->use_pipe[M_GRAD] = h->use_pipe[M_S2];
+    // fused stages 2+3 against the two chosen stage kernels
+    if (rc == SS_OK) {
+      A.mode = M_S23;
+      A.out_l = (R*)h->l[2];
+      A.out_l2 = (R*)h->l[1];
+      A.tm_l = h->tm[4];
+      A.with_energy = 0;
+      rc = launch(h, A, true);  // warm-up
+      if (rc == SS_OK) {
+        CK(cudaEventRecord(e0, h->stream));
+        for (int i = 0; i < iters && rc == SS_OK; ++i) rc = launch(h, A, true);
+        CK(cudaEventRecord(e1, h->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        h->tune_ms[M_S23][1] = ms / iters;
+        h->tune_ms[M_S23][0] = h->tune_ms[M_S2][h->use_pipe[M_S2]] + h->tune_ms[M_S3][h->use_pipe[M_S3]];
+        h->fuse23 = h->tune_ms[M_S23][1] <= h->tune_ms[M_S23][0] ? 1 : 0;
+      }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return rc;
@@ -886,7 +921,7 @@ int ss_autotune(ss_handle* h, int iters, float* ms_out) {
   });
   if (rc) return rc;
   if (ms_out)
-    for (int m = 0; m < 6; ++m) {
+    for (int m = 0; m < N_FLOW_MODES; ++m) {
       ms_out[2 * m] = h->tune_ms[m][0];
       ms_out[2 * m + 1] = h->tune_ms[m][1];
     }
@@ -902,15 +937,22 @@ int ss_debug_wait_timeout(ss_handle* h, long long wait_cycles, int inject) {
 }
 
 int ss_get_variant(const ss_handle* h, int mode) {
-  if (!h || mode < 0 || mode > 5) return -1;
+  if (!h || mode < 0 || mode > 6) return -1;
+  if (mode == M_S23) return h->fuse23;
   return h->use_pipe[mode];
 }
 
 int ss_set_variant(ss_handle* h, int mode, int variant) {
   if (!h) return fail(SS_ERR_ARG, "NULL handle");
-  if (mode < 0 || mode > 4) return fail(SS_ERR_ARG, "mode %d: 0 (gradient) or 1..4 (stages); the energy pass follows stage 1", mode);
+  if (mode < 0 || mode > 6 || mode == 5)
+    return fail(SS_ERR_ARG, "mode %d: 0 (gradient), 1..4 (stages) or 6 (stages 2+3 fused); the energy pass follows "
+                "stage 1", mode);
   if (variant != 0 && variant != 1) return fail(SS_ERR_ARG, "variant %d: 0 (one tile per CTA) or 1 (pipelined)", variant);
   if (h->precision == SS_PLAIN_FP64) return fail(SS_ERR_ARG, "the plain FP64 form has no staging variants");
+  if (mode == M_S23) {  // 1: stages 2 and 3 in one kernel (used with TMA staging), 0: two kernels
+    h->fuse23 = variant;
+    return SS_OK;
+  }
   if (variant == 1) {
     if (!h->tma) return fail(SS_ERR_STATE, "the pipelined variant needs TMA-staged buffers (bind first; rows of 16-byte multiples)");
     const bool ok = dispatch(h, [&](auto* tag) -> int {

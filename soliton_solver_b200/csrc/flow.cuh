@@ -27,7 +27,9 @@
 
 namespace ssb {
 
-enum FlowMode { M_GRAD = 0, M_S1 = 1, M_S2 = 2, M_S3 = 3, M_S4 = 4, M_ENERGY = 5 };
+// M_S23: stages 2 and 3 fused (one staging of phi, V, l1; writes l2 and l3)
+enum FlowMode { M_GRAD = 0, M_S1 = 1, M_S2 = 2, M_S3 = 3, M_S4 = 4, M_ENERGY = 5, M_S23 = 6 };
+constexpr int N_FLOW_MODES = 7;
 enum { ST_TIMEOUT = 6 };
 
 // Default bound of a device-side wait on an mbarrier (~1 s at 1.9 GHz).  On expiry
@@ -47,7 +49,8 @@ struct FlowArgs {
   const R* la;  // l1 (S3, S4)
   const R* lb;  // l2 (S4)
   const R* lc;  // l3 (S4)
-  R* out_l;     // S1..S3: l_s;  M_GRAD: l_out (nullable)
+  R* out_l;     // S1..S3: l_s;  M_S23: l3;  M_GRAD: l_out (nullable)
+  R* out_l2;    // M_S23: l2
   R* out_eg;    // M_GRAD: energy gradient (nullable)
   R* phi_out;   // S4
   R* vel_out;   // S4
@@ -91,7 +94,7 @@ __host__ __device__ constexpr size_t tile_buf_bytes() {
 
 // number of staged buffers a mode needs (phi, then velocity, then l)
 __host__ __device__ inline int flow_buffers(int mode) {
-  return mode == M_S2 ? 2 : (mode == M_S3 || mode == M_S4) ? 3 : 1;
+  return mode == M_S2 ? 2 : (mode == M_S3 || mode == M_S4 || mode == M_S23) ? 3 : 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -316,7 +319,7 @@ template <class TH, typename R, int TX, int TY, int NT, bool FAST, int MODE, boo
 __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, const R* Praw, const R* Vraw, int x0,
                                           int y0, bool arrest, double& err_max, const R* C1 = nullptr,
                                           const R* C3 = nullptr, double* e_acc = nullptr,
-                                          const typename PairOf<R>::type* L2c = nullptr) {
+                                          const typename PairOf<R>::type* L2c = nullptr, R* out_l = nullptr) {
   using TS = TileShape<TX, TY, NT>;
   using V = typename PairOf<R>::type;
   constexpr int NF = TH::NF;
@@ -412,8 +415,9 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
         if (A.out_l) gstore<V, R>(A.out_l + a * N + sidx, mdt * g[a], FAST, v1);
       }
     } else if constexpr (MODE != M_S4) {
+      R* const lo = out_l ? out_l : A.out_l;
 #pragma unroll
-      for (int a = 0; a < NF; ++a) gstore<V, R>(A.out_l + a * N + sidx, mdt * g[a], FAST, v1);
+      for (int a = 0; a < NF; ++a) gstore<V, R>(lo + a * N + sidx, mdt * g[a], FAST, v1);
     } else {
       // RK4 finalize (core/integrator.py:151-189) fused with stage 4:
       // V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,  phi' = phi + dt V + dt (l1 + l2 + l3)/6
@@ -560,7 +564,7 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   const int x0 = (tile / tiles_y) * TX;
   const int y0 = (tile % tiles_y) * TY;
   StepState* st = A.st;
-  constexpr bool uses_v = mode == M_S2 || mode == M_S3 || mode == M_S4;
+  constexpr bool uses_v = mode == M_S2 || mode == M_S3 || mode == M_S4 || mode == M_S23;
   // The arrest flag (set by the last block of stage 1) is read only after the TMA
   // copies are issued, so its global-memory round trip overlaps them.
   bool arrest = false;
@@ -576,7 +580,7 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   if constexpr (TMA) {
     // V is staged whether or not an arrest is pending (an arrested step ignores it)
     constexpr bool need_v = uses_v;
-    const bool need_l = mode == M_S3 || mode == M_S4;
+    const bool need_l = mode == M_S3 || mode == M_S4 || mode == M_S23;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -593,7 +597,21 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
       mbar_wait_bounded(&bar, 0, A.wait_cycles);
       return;
     }
-    if (mode == M_S2 || mode == M_S3 || mode == M_S4) {
+    if constexpr (mode == M_S23) {
+      // T3 = phi + dt/2 (V + l1/2) in place of l1 and T2 = phi + dt/2 V in place of V, in
+      // one pass (each element reads its own phi, V, l1 before writing)
+      using V = typename PairOf<R>::type;
+      const V half(0.5), hdt(grid_k<R>(G, GK_HDT));
+      for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
+        V p0, p1, v0(0.0), v1(0.0), w0, w1;
+        ld_quad(B0 + i, p0, p1);
+        if (!arrest) ld_quad(B1 + i, v0, v1);
+        ld_quad(B2 + i, w0, w1);
+        st_quad(B2 + i, vfma(hdt, vfma(half, w0, v0), p0), vfma(hdt, vfma(half, w1, v1), p1));
+        st_quad(B1 + i, vfma(hdt, v0, p0), vfma(hdt, v1, p1));
+      }
+      __syncthreads();
+    } else if (mode == M_S2 || mode == M_S3 || mode == M_S4) {
       // combine in place into the last staged buffer (OOB entries are zero in all)
       R* dst = need_l ? B2 : (need_v ? B1 : B0);
       if (dst != B0) {
@@ -643,6 +661,22 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   // exact FP64 differences of the staged values (energy_tile)
   constexpr bool JE = sizeof(R) == 4 && (MODE == M_S1 || MODE == M_ENERGY);
   const bool je = JE && !(MODE == M_ENERGY && A.exact_energy);
+  if constexpr (MODE == M_S23) {
+    // l3 from T3 (staged in B2), then l2 from T2 (staged in B1): the stage-3 and stage-2
+    // arithmetic per site, so the results equal the two separate stages bitwise
+    if (fast) {
+      grad_tile<TH, R, TX, TY, NT, true, M_S3>(A, B2, nullptr, nullptr, x0, y0, arrest, err_max, nullptr, nullptr,
+                                               nullptr, nullptr, A.out_l);
+      grad_tile<TH, R, TX, TY, NT, true, M_S2>(A, B1, nullptr, nullptr, x0, y0, arrest, err_max, nullptr, nullptr,
+                                               nullptr, nullptr, A.out_l2);
+    } else {
+      grad_tile<TH, R, TX, TY, NT, false, M_S3>(A, B2, nullptr, nullptr, x0, y0, arrest, err_max, nullptr, nullptr,
+                                                nullptr, nullptr, A.out_l);
+      grad_tile<TH, R, TX, TY, NT, false, M_S2>(A, B1, nullptr, nullptr, x0, y0, arrest, err_max, nullptr, nullptr,
+                                                nullptr, nullptr, A.out_l2);
+    }
+    return;
+  }
   if constexpr (MODE != M_ENERGY || JE) {
     if (MODE != M_ENERGY || je) {
       double* ep = (je && do_energy) ? &e_acc : nullptr;

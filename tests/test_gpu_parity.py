@@ -449,7 +449,8 @@ def test_pinned_variants_agree():
     p_i, p_f = theory.params.pack_device_params(rp)
     F = _smooth_field("chiral_magnet", rp, 9)
     outs = []
-    for v in (0, 1):
+    # (stage variant, stages 2+3 fused): all tile / all pipelined, fused and not
+    for v, fuse in ((0, 0), (1, 1), (0, 1), (1, 0)):
         s = Solver(0, p_i, p_f, "fp32")
         f, vel = _dev(F, "fp32"), _dev(np.zeros_like(F), "fp32")
         s.bind(f, vel)
@@ -457,11 +458,14 @@ def test_pinned_variants_agree():
             s.set_variant(m, v)
             assert s._lib.ss_get_variant(s._h, m) == v
         assert s._lib.ss_get_variant(s._h, 5) == v  # the energy pass follows stage 1
+        s.set_variant(6, fuse)
+        assert s._lib.ss_get_variant(s._h, 6) == fuse
         E, _ = s.step(6, 1e300)
         outs.append((E, f.cpu().numpy(), vel.cpu().numpy()))
-    np.testing.assert_array_equal(outs[0][1], outs[1][1])
-    np.testing.assert_array_equal(outs[0][2], outs[1][2])
-    np.testing.assert_allclose(outs[0][0], outs[1][0], rtol=1e-12)
+    for E, f, vel in outs[1:]:
+        np.testing.assert_array_equal(f, outs[0][1])
+        np.testing.assert_array_equal(vel, outs[0][2])
+        np.testing.assert_allclose(E, outs[0][0], rtol=1e-12)
     for bad in ((5, 0), (1, 2), (-1, 0)):
         with pytest.raises(ValueError):
             s.set_variant(*bad)
