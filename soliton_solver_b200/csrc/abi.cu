@@ -1403,7 +1403,7 @@ size_t batch_layout(ss_batch* b, char* base) {
 template <class TH, typename R>
 struct Batched {
   static constexpr size_t BUF = tile_buf_bytes<R, TH::NF, TX, TY>();
-  static inline unsigned long long smem_done[2][6] = {};
+  static inline unsigned long long smem_done[2][N_FLOW_MODES] = {};
 
   template <bool TMA_, int MODE>
   static int launch_mode(const ss_batch* b, const BatchStep& B) {
@@ -1437,8 +1437,12 @@ struct Batched {
       B.with_energy = B.arrest_update = B.init_state = 0;
       B.prev_energy = nullptr;
       B.E_idx = -1;
-      if ((rc = launch<M_S2>(b, B))) return rc;
-      if ((rc = launch<M_S3>(b, B))) return rc;
+      if (b->tma) {  // stages 2 and 3 fused (one staging of phi, V, l1)
+        if ((rc = launch_mode<true, M_S23>(b, B))) return rc;
+      } else {
+        if ((rc = launch<M_S2>(b, B))) return rc;
+        if ((rc = launch<M_S3>(b, B))) return rc;
+      }
       B.err_idx = s;
       if ((rc = launch<M_S4>(b, B))) return rc;
       B.err_idx = -1;

@@ -55,7 +55,9 @@ __global__ void __launch_bounds__(NT)
     A.la = (const R*)I.buf[4];
     A.lb = (const R*)I.buf[5];
     A.lc = (const R*)I.buf[6];
-    A.out_l = MODE == M_S1 ? (R*)I.buf[4] : MODE == M_S2 ? (R*)I.buf[5] : MODE == M_S3 ? (R*)I.buf[6] : nullptr;
+    A.out_l = MODE == M_S1 ? (R*)I.buf[4] : MODE == M_S2 ? (R*)I.buf[5] : (MODE == M_S3 || MODE == M_S23)
+                                                                            ? (R*)I.buf[6] : nullptr;
+    A.out_l2 = MODE == M_S23 ? (R*)I.buf[5] : nullptr;
     A.out_eg = nullptr;
     A.phi_out = (R*)I.buf[cur ? 0 : 2];
     A.vel_out = (R*)I.buf[cur ? 1 : 3];
@@ -76,7 +78,8 @@ __global__ void __launch_bounds__(NT)
     A.tx_extra = 0;
   }
   __syncthreads();
-  flow_tile<TH, R, TX, TY, NT, TMA, MODE>(A, &I.tm[cur ? 2 : 0], &I.tm[cur ? 3 : 1], &I.tm[MODE == M_S3 ? 4 : 5],
+  flow_tile<TH, R, TX, TY, NT, TMA, MODE>(A, &I.tm[cur ? 2 : 0], &I.tm[cur ? 3 : 1],
+                                          &I.tm[(MODE == M_S3 || MODE == M_S23) ? 4 : 5],
                                           blockIdx.x - I.tile0, I.ntiles, smem_raw, S);
 }
 
