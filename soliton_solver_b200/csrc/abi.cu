@@ -445,6 +445,11 @@ struct Fused {
     // maps: [0] field [1] velocity [2] phi_alt [3] vel_alt [4] l1 [5] l2
     int cur = 0;
     for (int s = 0; s < n; ++s) {
+      // The last step of a call with an odd count reads the caller's buffers and would
+      // leave its result in the alternates (a copy back after the call).  Instead stage 2
+      // copies phi and V into the alternates on its way (it stages both anyway) and stage
+      // 4 reads them there and writes the result into the caller's buffers.
+      const bool land = s == n - 1 && cur == 0;
       A.phi = cur_p;
       A.vel = cur_v;
       if (tma) {
@@ -467,7 +472,13 @@ struct Fused {
       A.E_idx = -1;
       // S2, S3: one fused kernel on TMA-staged buffers (one staging of phi, V, l1),
       // else two
-      if (tma && h->fuse23) {
+      const bool fused23 = tma && h->fuse23;
+      const bool copy_in_s2 = land && (fused23 || !tma || !h->use_pipe[M_S2]);  // one tile per CTA
+      if (copy_in_s2) {
+        A.copy_phi = alt_p;
+        A.copy_vel = alt_v;
+      }
+      if (fused23) {
         A.mode = M_S23;
         A.la = l1;
         A.out_l = l3;
@@ -479,11 +490,28 @@ struct Fused {
         A.mode = M_S2;
         A.out_l = l2;
         if ((rc = launch(h, A, tma))) return rc;
+        A.copy_phi = nullptr;
+        A.copy_vel = nullptr;
         A.mode = M_S3;
         A.la = l1;
         A.out_l = l3;
         if (tma) A.tm_l = h->tm[4];
         if ((rc = launch(h, A, tma))) return rc;
+      }
+      A.copy_phi = nullptr;
+      A.copy_vel = nullptr;
+      const size_t bytes = (size_t)h->nf * h->G.N * sizeof(R);
+      if (land && !copy_in_s2) {  // pipelined stage 2: plain copies
+        CK(cudaMemcpyAsync(alt_p, cur_p, bytes, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(alt_v, cur_v, bytes, cudaMemcpyDeviceToDevice, h->stream));
+      }
+      if (land) {  // stage 4 reads phi and V from the alternates, writes the caller's buffers
+        A.phi = alt_p;
+        A.vel = alt_v;
+        if (tma) {
+          A.tm_phi = h->tm[2];
+          A.tm_vel = h->tm[3];
+        }
       }
       // S4 + finalize into the ping-pong buffers
       A.mode = M_S4;
@@ -491,8 +519,8 @@ struct Fused {
       A.lb = l2;
       A.lc = l3;
       A.out_l = nullptr;
-      A.phi_out = alt_p;
-      A.vel_out = alt_v;
+      A.phi_out = land ? cur_p : alt_p;
+      A.vel_out = land ? cur_v : alt_v;
       A.err_idx = s;
       if (tma) {
         A.tm_l = h->tm[5];
@@ -501,9 +529,11 @@ struct Fused {
       }
       if ((rc = launch(h, A, tma))) return rc;
       A.err_idx = -1;
-      std::swap(cur_p, alt_p);
-      std::swap(cur_v, alt_v);
-      cur ^= 1;
+      if (!land) {
+        std::swap(cur_p, alt_p);
+        std::swap(cur_v, alt_v);
+        cur ^= 1;
+      }
     }
     // trailing energy of the final field + arrest test
     A.phi = cur_p;

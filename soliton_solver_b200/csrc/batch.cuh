@@ -61,6 +61,8 @@ __global__ void __launch_bounds__(NT)
     A.out_eg = nullptr;
     A.phi_out = (R*)I.buf[cur ? 0 : 2];
     A.vel_out = (R*)I.buf[cur ? 1 : 3];
+    A.copy_phi = nullptr;
+    A.copy_vel = nullptr;
     A.partial = I.partial;
     A.st = I.st;
     A.E_traj = I.E_traj;

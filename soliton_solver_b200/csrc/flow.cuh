@@ -54,6 +54,8 @@ struct FlowArgs {
   R* out_eg;    // M_GRAD: energy gradient (nullable)
   R* phi_out;   // S4
   R* vel_out;   // S4
+  R* copy_phi;  // S2 / M_S23, one tile per CTA (nullable): copy of phi's and V's centres, so
+  R* copy_vel;  //   that this step's S4 can read them there and write into phi / vel
   double* partial;  // per-block energy partials
   StepState* st;
   double* E_traj;   // nullable
@@ -86,6 +88,25 @@ struct TileShape {
   static_assert(NT % TY == 0 && TX % (NT / TY) == 0, "tile/thread mismatch");
   static_assert(TY % 4 == 0, "TY must keep the y start 16-byte aligned");
 };
+
+// Centre of a tile (TX x TY sites, NF components) of phi and V into A.copy_phi /
+// A.copy_vel, from the staged halo tiles Pt / Vt (phi and V as loaded) or, when those
+// are null, from A.phi / A.vel.  Rows of TY consecutive values: coalesced stores.
+template <int NF, typename R, int TX, int TY, int NT, typename FA>
+__device__ __forceinline__ void copy_centre(const FA& A, const R* Pt, const R* Vt, int x0, int y0) {
+  using TS = TileShape<TX, TY, NT>;
+  const Grid& G = A.G;
+#pragma unroll 4
+  for (int i = threadIdx.x; i < NF * TX * TY; i += NT) {
+    const int y = i % TY, lx = (i / TY) % TX, a = i / (TX * TY);
+    const int gx = x0 + lx, gy = y0 + y;
+    if (gx >= G.X || gy >= G.Y) continue;
+    const long long g = a * G.N + (long long)gx * G.Y + gy;
+    const int t = a * TS::PLANE + (lx + 2) * TS::HY + TS::YOFF + y;
+    A.copy_phi[g] = Pt ? Pt[t] : A.phi[g];
+    A.copy_vel[g] = Vt ? Vt[t] : A.vel[g];
+  }
+}
 
 template <typename R, int NF, int TX, int TY>
 __host__ __device__ constexpr size_t tile_buf_bytes() {
@@ -597,6 +618,12 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
       mbar_wait_bounded(&bar, 0, A.wait_cycles);
       return;
     }
+    if constexpr (mode == M_S2 || mode == M_S23) {
+      if (A.copy_phi) {  // uniform over the block
+        copy_centre<NF, R, TX, TY, NT>(A, B0, B1, x0, y0);
+        __syncthreads();  // every value is copied before the combine overwrites V in place
+      }
+    }
     if constexpr (mode == M_S23) {
       // T3 = phi + dt/2 (V + l1/2) in place of l1 and T2 = phi + dt/2 V in place of V, in
       // one pass (each element reads its own phi, V, l1 before writing)
@@ -642,6 +669,9 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   } else {
     if constexpr (uses_v) arrest = st->arrest != 0;
     stage_plain<NF, R, TX, TY, NT>(B0, A, x0, y0, mode, arrest);
+    if constexpr (mode == M_S2) {
+      if (A.copy_phi) copy_centre<NF, R, TX, TY, NT>(A, (const R*)nullptr, (const R*)nullptr, x0, y0);
+    }
     __syncthreads();
   }
 
