@@ -110,7 +110,10 @@ int ss_bind(ss_handle *h, void *field, void *velocity, void *workspace, size_t w
  * energy_traj[s] / err_traj[s] (host, nullable) receive E after step s and the
  * signed maximum of the stage-4 energy gradient of step s.  prev_energy is the
  * energy the first step's arrest test compares against; pass NaN to continue from
- * the energy the previous ss_step call left on the device. */
+ * the energy the previous ss_step call left on the device.  Steps run in chunks of
+ * 1024; a non-finite energy or a timed-out wait ends the call after the chunk in
+ * which it happened (the trajectories up to there are written).  The first call
+ * page-locks a 16 KB host staging buffer, held until ss_destroy. */
 int ss_step(ss_handle *h, int n_steps, double prev_energy, double *energy_traj, double *err_traj);
 /* As ss_step but without a host synchronisation: the trajectories go to device
  * arrays of n_steps doubles (nullable) and the status of the device-side checks is

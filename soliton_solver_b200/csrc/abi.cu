@@ -124,8 +124,12 @@ struct ss_handle {
   long long wait_cycles = WAIT_CYCLES;
   mutable int inject_timeout = 0;  // test hook, consumed by the next flow launch
   cudaGraphExec_t graph = nullptr;  // captured n-step relaxation (ss_graph_create)
+  // page-locked host staging of ss_step: energy and err trajectories of one chunk and
+  // the StepState, copied with one synchronisation (allocated on the first ss_step)
+  double* host_stage = nullptr;
   ~ss_handle() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (host_stage) cudaFreeHost(host_stage);
   }
 };
 
@@ -787,19 +791,21 @@ int read_state(ss_handle* h, StepState* out) {
   return SS_OK;
 }
 
+// error of a nonzero device status (read by the caller), which is cleared on the device
+int status_error(ss_handle* h, int status) {
+  const int zero = 0;
+  CK(cudaMemcpyAsync(&h->st->status, &zero, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (status == SS_ERR_TIMEOUT)
+    return fail(SS_ERR_TIMEOUT, "a device-side wait timed out; re-bind the handle before further use");
+  return fail(SS_ERR_NONFINITE, "a reduction produced a non-finite value");
+}
+
 int take_status(ss_handle* h) {
   StepState s;
   int rc = read_state(h, &s);
   if (rc) return rc;
-  if (s.status) {
-    const int zero = 0;
-    CK(cudaMemcpyAsync(&h->st->status, &zero, sizeof(int), cudaMemcpyHostToDevice, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    if (s.status == SS_ERR_TIMEOUT)
-      return fail(SS_ERR_TIMEOUT, "a device-side wait timed out; re-bind the handle before further use");
-    return fail(SS_ERR_NONFINITE, "a reduction produced a non-finite value");
-  }
-  return SS_OK;
+  return s.status ? status_error(h, s.status) : SS_OK;
 }
 
 int fused_density(ss_handle* h, const void* field, double* dens, bool reduce, int kind, int which) {
@@ -897,7 +903,8 @@ int ss_destroy(ss_handle* h) {
 int ss_workspace_bytes(const ss_handle* h, size_t* bytes) {
   if (!h || !bytes) return fail(SS_ERR_ARG, "NULL argument");
   ss_handle tmp = *h;
-  tmp.graph = nullptr;  // the copy must not own the original's graph
+  tmp.graph = nullptr;  // the copy must not own the original's graph or staging
+  tmp.host_stage = nullptr;
   *bytes = layout(&tmp, nullptr);
   return SS_OK;
 }
@@ -1021,18 +1028,30 @@ int ss_step(ss_handle* h, int n_steps, double prev_energy, double* energy_traj, 
       return Plain<TH>::step(h, n_steps, prev_energy, energy_traj, err_traj);
     });
   }
+  if (n_steps == 0) return take_status(h);
+  // each chunk's trajectories and the device state come back through page-locked
+  // staging: the copies queue behind the kernels and one synchronisation waits for all
+  if (!h->host_stage)
+    CK(cudaHostAlloc((void**)&h->host_stage, 2 * TRAJ_CAP * sizeof(double) + sizeof(StepState),
+                     cudaHostAllocDefault));
+  double* hE = h->host_stage;
+  double* hErr = h->host_stage + TRAJ_CAP;
+  StepState* hs = reinterpret_cast<StepState*>(h->host_stage + 2 * TRAJ_CAP);
   double prev = prev_energy;
   for (int done = 0; done < n_steps; done += TRAJ_CAP) {
     const int k = std::min(TRAJ_CAP, n_steps - done);
     rc = ss_step_async(h, k, prev, h->traj_E, h->traj_err);
     if (rc) return rc;
     prev = NAN;
-    if (energy_traj)
-      CK(cudaMemcpyAsync(energy_traj + done, h->traj_E, k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    if (err_traj)
-      CK(cudaMemcpyAsync(err_traj + done, h->traj_err, k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (energy_traj) CK(cudaMemcpyAsync(hE, h->traj_E, k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (err_traj) CK(cudaMemcpyAsync(hErr, h->traj_err, k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(hs, h->st, sizeof(StepState), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (energy_traj) memcpy(energy_traj + done, hE, k * sizeof(double));
+    if (err_traj) memcpy(err_traj + done, hErr, k * sizeof(double));
+    if (hs->status) return status_error(h, hs->status);
   }
-  return take_status(h);
+  return SS_OK;
 }
 
 int ss_check_status(ss_handle* h) {
