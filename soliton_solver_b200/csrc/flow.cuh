@@ -1007,8 +1007,9 @@ __global__ void __launch_bounds__(NT, (pipe_ctas<TH, MODE>())) flow_kernel_pipe(
   }
 }
 
-// Copy the ping-pong result back into the caller's buffers (when the step count
-// was odd) and apply a pending arrest (V = 0) left by the trailing energy pass.
+// Apply a pending arrest (V = 0) left by the trailing energy pass, and copy the result
+// back into the caller's buffers when `copy` says it sits in the alternates (the fused
+// step never leaves it there: the last step of an odd count writes the caller's buffers).
 template <typename R>
 __global__ void finish_kernel(const R* __restrict__ phi_src, const R* __restrict__ vel_src, R* phi_dst,
                               R* vel_dst, long long n, int copy, const StepState* st) {
