@@ -404,7 +404,10 @@ struct Fused {
       h->inject_timeout = 0;
     }
     if (!tma) return launch_tma<false>(h, A);
-    if (!h->use_pipe[A.mode]) return launch_tma<true>(h, A);
+    // exact FP64 energies (observables) run one tile per CTA: the pipelined energy pass
+    // of the packed-energy theories is built for the flow energy only
+    if (!h->use_pipe[A.mode] || (A.mode == M_ENERGY && A.exact_energy && pipe_ctas<TH, M_ENERGY>() == 4))
+      return launch_tma<true>(h, A);
     switch (A.mode) {
       case M_GRAD: return launch_pipe<M_GRAD>(h, A);
       case M_S1: return launch_pipe<M_S1>(h, A);

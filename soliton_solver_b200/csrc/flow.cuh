@@ -940,7 +940,10 @@ __global__ void __launch_bounds__(NT, (pipe_ctas<TH, MODE>())) flow_kernel_pipe(
     const bool fast = (G.Y % 2 == 0) && x0 >= G.halo + 1 && x0 + TX - 1 <= G.X - G.halo - 2 &&
                       y0 >= G.halo + 1 && y0 + TY - 1 <= G.Y - G.halo - 2;
     constexpr bool JE = sizeof(R) == 4 && (MODE == M_S1 || MODE == M_ENERGY);
-    const bool je = JE && !(MODE == M_ENERGY && A.exact_energy);
+    // the four-CTA energy pass is built for the flow energy only (the exact FP64 energy
+    // would spill out of its 64 registers); the host sends exact energies to flow_kernel
+    constexpr bool EXACT = !(MODE == M_ENERGY && pipe_ctas<TH, MODE>() == 4);
+    const bool je = JE && !(MODE == M_ENERGY && EXACT && A.exact_energy);
     if constexpr (MODE != M_ENERGY || JE) {
       if (MODE != M_ENERGY || je) {
         double* ep = (je && do_energy) ? &e_acc : nullptr;
@@ -952,7 +955,7 @@ __global__ void __launch_bounds__(NT, (pipe_ctas<TH, MODE>())) flow_kernel_pipe(
                                                        L2REG ? l2c : nullptr);
       }
     }
-    if constexpr (MODE == M_S1 || MODE == M_ENERGY) {
+    if constexpr ((MODE == M_S1 || MODE == M_ENERGY) && EXACT) {
       if (do_energy && !je) {
         if (fast)
           e_acc += energy_tile<TH, R, TX, TY, NT, true>(A, T, x0, y0);
