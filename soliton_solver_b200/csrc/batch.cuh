@@ -31,8 +31,17 @@ struct BatchStep {
   long long wait_cycles;
 };
 
+// Resident CTAs per SM the batched stage kernels are built for.  Each CTA stages,
+// computes and stores one tile, so the staging latency is hidden only by other
+// resident CTAs: FP32 fields cap the registers for three (85 per thread) instead of
+// the two that the heavier stencils (the Baby Skyrme term) would otherwise get.
+template <typename R, int MODE>
+__host__ __device__ constexpr int batch_ctas() {
+  return sizeof(R) == 4 ? 3 : 1;
+}
+
 template <class TH, typename R, int TX, int TY, int NT, bool TMA, int MODE>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, (batch_ctas<R, MODE>()))
     batch_flow_kernel(const BatchInst* __restrict__ insts, const int* __restrict__ tile_inst,
                       const __grid_constant__ BatchStep B) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -40,6 +49,20 @@ __global__ void __launch_bounds__(NT)
   __shared__ FlowArgs<R> A;
   const int inst = tile_inst[blockIdx.x];
   const BatchInst& I = insts[inst];
+  const int cur = B.parity;
+  const CUtensorMap* tm_phi = &I.tm[cur ? 2 : 0];
+  const CUtensorMap* tm_vel = &I.tm[cur ? 3 : 1];
+  const CUtensorMap* tm_l = &I.tm[(MODE == M_S3 || MODE == M_S23) ? 4 : 5];
+  if constexpr (TMA) {
+    // the tile's loads first, so the set-up below overlaps them
+    if (threadIdx.x == 0) {
+      const int tile = blockIdx.x - I.tile0;
+      const int tiles_y = (I.G.Y + TY - 1) / TY;
+      mbar_init(&S.bar, 1);
+      issue_tile<TH, R, TX, TY, NT, MODE>(reinterpret_cast<R*>(smem_raw), tm_phi, tm_vel, tm_l, (tile / tiles_y) * TX,
+                                          (tile % tiles_y) * TY, &S.bar, 0u);
+    }
+  }
   {  // the lattice's parameters into shared memory (word copy)
     const int* src = reinterpret_cast<const int*>(&I.G);
     int* dst = reinterpret_cast<int*>(&A.G);
@@ -48,7 +71,6 @@ __global__ void __launch_bounds__(NT)
     dst = reinterpret_cast<int*>(&A.P);
     for (int i = threadIdx.x; i < (int)(sizeof(Phys) / 4); i += NT) dst[i] = src[i];
   }
-  const int cur = B.parity;
   if (threadIdx.x == 0) {
     A.phi = (const R*)I.buf[cur ? 2 : 0];
     A.vel = (const R*)I.buf[cur ? 3 : 1];
@@ -80,9 +102,7 @@ __global__ void __launch_bounds__(NT)
     A.tx_extra = 0;
   }
   __syncthreads();
-  flow_tile<TH, R, TX, TY, NT, TMA, MODE>(A, &I.tm[cur ? 2 : 0], &I.tm[cur ? 3 : 1],
-                                          &I.tm[(MODE == M_S3 || MODE == M_S23) ? 4 : 5],
-                                          blockIdx.x - I.tile0, I.ntiles, smem_raw, S);
+  flow_tile<TH, R, TX, TY, NT, TMA, MODE>(A, tm_phi, tm_vel, tm_l, blockIdx.x - I.tile0, I.ntiles, smem_raw, S, TMA);
 }
 
 // Copy each lattice's result back into the caller's buffers when the alternates hold

@@ -552,6 +552,25 @@ __device__ __forceinline__ double energy_tile(const FlowArgs<R>& A, const E* T, 
   return e_acc + (double)(Lanes<V>::get(chk, 0) + Lanes<V>::get(chk, 1));
 }
 
+// Expect and issue the TMA loads of one tile's staged buffers (called by one thread,
+// after the barrier is initialised): phi into B0, and V into B0 + BUF and the mode's l
+// buffer into B0 + 2 BUF where the mode combines them.  V is staged whether or not an
+// arrest is pending (an arrested step ignores it).
+template <class TH, typename R, int TX, int TY, int NT, int MODE>
+__device__ __forceinline__ void issue_tile(R* B0, const CUtensorMap* tm_phi, const CUtensorMap* tm_vel,
+                                           const CUtensorMap* tm_l, int x0, int y0, uint64_t* bar,
+                                           unsigned tx_extra) {
+  using TS = TileShape<TX, TY, NT>;
+  constexpr int BUF = TH::NF * TS::PLANE;
+  constexpr bool need_v = MODE == M_S2 || MODE == M_S3 || MODE == M_S4 || MODE == M_S23;
+  constexpr bool need_l = MODE == M_S3 || MODE == M_S4 || MODE == M_S23;
+  constexpr uint32_t bytes = (uint32_t)(sizeof(R) * BUF) * (1u + (need_v ? 1u : 0u) + (need_l ? 1u : 0u));
+  mbar_expect_tx(bar, bytes + tx_extra);
+  tma_load_3d(B0, tm_phi, y0 - TS::YOFF, x0 - 2, 0, bar);
+  if constexpr (need_v) tma_load_3d(B0 + BUF, tm_vel, y0 - TS::YOFF, x0 - 2, 0, bar);
+  if constexpr (need_l) tma_load_3d(B0 + 2 * BUF, tm_l, y0 - TS::YOFF, x0 - 2, 0, bar);
+}
+
 // Shared scratch of the one-tile-per-CTA stage kernels besides the staged tile.
 template <int NT>
 struct StageShared {
@@ -563,10 +582,12 @@ struct StageShared {
 
 // Stage, compute and reduce tile `tile` of a lattice of `nblk` tiles (one CTA per
 // tile).  tm_phi / tm_vel / tm_l are TMA maps in parameter or global memory.
+// issued: thread 0 has already initialised S.bar and issued the tile's loads
+// (issue_tile), so the caller's set-up overlapped them.
 template <class TH, typename R, int TX, int TY, int NT, bool TMA, int MODE>
 __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMap* tm_phi, const CUtensorMap* tm_vel,
                                           const CUtensorMap* tm_l, int tile, int nblk, unsigned char* smem_raw,
-                                          StageShared<NT>& S) {
+                                          StageShared<NT>& S, bool issued = false) {
   using TS = TileShape<TX, TY, NT>;
   constexpr int NF = TH::NF;
   constexpr int BUF = NF * TS::PLANE;
@@ -599,17 +620,12 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   // ---- stage the halo tile of T_s --------------------------------------
   R* T = B0;
   if constexpr (TMA) {
-    // V is staged whether or not an arrest is pending (an arrested step ignores it)
     constexpr bool need_v = uses_v;
     const bool need_l = mode == M_S3 || mode == M_S4 || mode == M_S23;
-    if (threadIdx.x == 0) mbar_init(&bar, 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const uint32_t bytes = (uint32_t)(sizeof(R) * BUF) * (1u + (need_v ? 1u : 0u) + (need_l ? 1u : 0u));
-      mbar_expect_tx(&bar, bytes + A.tx_extra);
-      tma_load_3d(B0, tm_phi, y0 - TS::YOFF, x0 - 2, 0, &bar);
-      if (need_v) tma_load_3d(B1, tm_vel, y0 - TS::YOFF, x0 - 2, 0, &bar);
-      if (need_l) tma_load_3d(B2, tm_l, y0 - TS::YOFF, x0 - 2, 0, &bar);
+    if (!issued) {
+      if (threadIdx.x == 0) mbar_init(&bar, 1);
+      __syncthreads();
+      if (threadIdx.x == 0) issue_tile<TH, R, TX, TY, NT, MODE>(B0, tm_phi, tm_vel, tm_l, x0, y0, &bar, A.tx_extra);
     }
     if constexpr (uses_v) arrest = st->arrest != 0;
     const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0, A.wait_cycles));
