@@ -1478,6 +1478,10 @@ struct Batched {
     B.wait_cycles = b->wait_cycles;
     int parity = 0, rc;
     for (int s = 0; s < n; ++s) {
+      // the last step of an odd count ends in the caller's buffers: stage 2 copies phi
+      // and V into the alternates and stage 4 runs at parity 1 (reads the alternates,
+      // writes the caller's buffers), so no copy back follows
+      const bool land = s == n - 1 && parity == 0;
       B.parity = parity;
       B.with_energy = s > 0;
       B.arrest_update = s > 0;
@@ -1489,16 +1493,20 @@ struct Batched {
       B.with_energy = B.arrest_update = B.init_state = 0;
       B.prev_energy = nullptr;
       B.E_idx = -1;
+      B.copy_out = land;
       if (b->tma) {  // stages 2 and 3 fused (one staging of phi, V, l1)
         if ((rc = launch_mode<true, M_S23>(b, B))) return rc;
       } else {
         if ((rc = launch<M_S2>(b, B))) return rc;
+        B.copy_out = 0;
         if ((rc = launch<M_S3>(b, B))) return rc;
       }
+      B.copy_out = 0;
       B.err_idx = s;
+      if (land) B.parity = 1;
       if ((rc = launch<M_S4>(b, B))) return rc;
       B.err_idx = -1;
-      parity ^= 1;
+      if (!land) parity ^= 1;
     }
     B.parity = parity;
     B.with_energy = B.arrest_update = 1;

@@ -25,6 +25,8 @@ struct BatchInst {
 
 struct BatchStep {
   int parity;         // 0: the caller's buffers hold the current field; 1: the alternates do
+  int copy_out;       // S2 / M_S23 at parity 0: also copy phi's and V's centres into the
+                      // alternates (the last step of an odd count; its S4 runs at parity 1)
   int with_energy, arrest_update, init_state;
   int E_idx, err_idx;
   const double* prev_energy;  // device, one per lattice (NaN keeps E_last); read with init_state
@@ -83,8 +85,9 @@ __global__ void __launch_bounds__(NT, (batch_ctas<R, MODE>()))
     A.out_eg = nullptr;
     A.phi_out = (R*)I.buf[cur ? 0 : 2];
     A.vel_out = (R*)I.buf[cur ? 1 : 3];
-    A.copy_phi = nullptr;
-    A.copy_vel = nullptr;
+    const bool copy = (MODE == M_S2 || MODE == M_S23) && B.copy_out;
+    A.copy_phi = copy ? (R*)I.buf[2] : nullptr;
+    A.copy_vel = copy ? (R*)I.buf[3] : nullptr;
     A.partial = I.partial;
     A.st = I.st;
     A.E_traj = I.E_traj;

@@ -66,6 +66,40 @@ def test_batch_matches_single_lattices(precision, aligned):
     assert np.all(np.isfinite(E2))
 
 
+@pytest.mark.parametrize("aligned", [True, False], ids=["tma", "plain"])
+def test_batch_odd_step_counts_are_bitwise_invariant(aligned):
+    """The last step of an odd-count batched call ends in the caller's buffers (stage 2
+    copies phi and V into the alternates, stage 4 runs at the opposite parity): seven
+    steps split into odd and even calls equal one call bitwise, arrests included."""
+    th = load_theory("Baby Skyrme")
+    sizes = [s for s in SIZES if (s[1] % 4 == 0) == aligned]
+    rng = np.random.default_rng(11)
+    params = [th.params.default_params(xlen=X, ylen=Y, lsx=0.1, lsy=0.1, time_step=0.02,
+                                       kappa=float(rng.uniform(0.5, 2)), mpi=float(rng.uniform(0.5, 2)),
+                                       unit_magnetization=True) for X, Y in sizes]
+    fields = [_hedgehog(p.resolved(), B=i % 4 + 1, R=float(rng.uniform(1, 3)), seed=i) for i, p in enumerate(params)]
+    prev = np.full(len(sizes), 1e300)
+    prev[0] = -1e300  # arrest fires for this lattice
+    outs = []
+    for split in ([7], [1, 2, 1, 3], [3, 3, 1]):
+        b = BatchSolver(th, params, "fp32")
+        assert b.tma_enabled == aligned
+        for i, F in enumerate(fields):
+            b.load(i, F)
+        Es = []
+        for j, k in enumerate(split):
+            E, _ = b.step(k, prev if j == 0 else None)
+            Es.append(E)
+        outs.append((np.concatenate(Es, axis=1), [f.cpu().numpy() for f in b.fields],
+                     [v.cpu().numpy() for v in b.velocities]))
+    for E, fs, vs in outs[1:]:
+        np.testing.assert_array_equal(E, outs[0][0])
+        for a, c in zip(fs, outs[0][1]):
+            np.testing.assert_array_equal(a, c)
+        for a, c in zip(vs, outs[0][2]):
+            np.testing.assert_array_equal(a, c)
+
+
 def test_batch_sweep_config_shape():
     """256 lattices with sizes from {64, 128, 256, 512}^2, random couplings and charges
     (the batched baby Skyrme sweep), FP32: runs and keeps every energy finite and each
