@@ -532,6 +532,36 @@ def dat_field_dump(dev, F0, reps=3):
             "note": "ss_format_text incl. its length pass, scan and one stream sync; wall clock"}
 
 
+def fused_fp64(dev, F0, steps=50):
+    """The same lattice with FP64 fields through the fused stage kernels (autotuned):
+    the precision-matched comparison with the plain FP64 form."""
+    import torch
+    from soliton_solver_b200.core.simulation import Simulation
+    th, p = chiral_params()
+    sim = Simulation(p, th, precision="fp64", device=dev)
+    sim.load_field(F0)
+    s = sim.solver
+    s.autotune(3)
+    s.step(3, 1e300)
+    E = torch.empty(steps, dtype=torch.float64, device=dev)
+    err = torch.empty(steps, dtype=torch.float64, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    s.step_async(steps, math.nan, E, err)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    words = WORDS_FUSED if (s.tma_enabled and s._lib.ss_get_variant(s._h, 6) == 1) else WORDS_SEPARATE
+    gbs = words * 4 * 8 * XLEN * YLEN / (ms / 1e3) / 1e9
+    out = {"value": XLEN * YLEN / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms, "steps": steps,
+           "achieved_gbs": gbs, "bytes_per_point_update": words * 4 * 8, "finite": bool(torch.isfinite(E).all()),
+           "note": "FP64 fields, fused stage kernels, same lattice; CUDA events"}
+    del sim
+    torch.cuda.empty_cache()
+    return out
+
+
 def compare_fp64_and_plain(args, dev, F0):
     """Relaxed-state accuracy (320^2), and the plain-FP64 form's speed on this lattice."""
     import torch
@@ -545,6 +575,10 @@ def compare_fp64_and_plain(args, dev, F0):
             out[key] = fn(dev)
         except Exception as exc:  # reported, not fatal: the headline line must still print
             out[key] = {"error": f"{type(exc).__name__}: {exc}"}
+    try:
+        out["fused_fp64"] = fused_fp64(dev, F0)
+    except Exception as exc:
+        out["fused_fp64"] = {"error": f"{type(exc).__name__}: {exc}"}
     sim = Simulation(p, th, precision="plain_fp64", device=dev)
     sim.load_field(F0)
     sim.relax(1, 1e300)
