@@ -325,12 +325,20 @@ struct Fused {
     return TMA_ ? flow_buffers(MODE) * BUF : BUF;
   }
 
+  // threads of a one-tile CTA: 512 where the staged buffers leave room for only one CTA
+  // per SM (FP64 stages 3, 4 and 2+3, the six-component s+id in FP64), else 256
+  template <bool TMA_, int MODE>
+  static constexpr int flow_threads() {
+    return flow_smem<TMA_, MODE>() > 113 * 1024 ? 2 * NT : NT;
+  }
+
   template <bool TMA_, int MODE>
   static int launch_mode(const ss_handle* h, const FlowArgs<R>& A) {
-    auto k = flow_kernel<TH, R, TX, TY, NT, TMA_, MODE>;
+    constexpr int NTM = flow_threads<TMA_, MODE>();
+    auto k = flow_kernel<TH, R, TX, TY, NTM, TMA_, MODE>;
     const size_t smem = flow_smem<TMA_, MODE>();
     set_smem(k, smem, smem_done[TMA_ ? 1 : 0][MODE]);
-    k<<<h->nblocks, NT, smem, h->stream>>>(A);
+    k<<<h->nblocks, NTM, smem, h->stream>>>(A);
     CK(cudaGetLastError());
     return SS_OK;
   }
@@ -1459,10 +1467,11 @@ struct Batched {
 
   template <bool TMA_, int MODE>
   static int launch_mode(const ss_batch* b, const BatchStep& B) {
-    auto k = batch_flow_kernel<TH, R, TX, TY, NT, TMA_, MODE>;
-    const size_t smem = TMA_ ? flow_buffers(MODE) * BUF : BUF;
+    constexpr size_t smem = TMA_ ? flow_buffers(MODE) * BUF : BUF;
+    constexpr int NTM = smem > 113 * 1024 ? 2 * NT : NT;  // as Fused::flow_threads
+    auto k = batch_flow_kernel<TH, R, TX, TY, NTM, TMA_, MODE>;
     set_smem(k, smem, smem_done[TMA_ ? 1 : 0][MODE]);
-    k<<<b->total_tiles, NT, smem, b->stream>>>(b->d_insts, b->d_tile_inst, B);
+    k<<<b->total_tiles, NTM, smem, b->stream>>>(b->d_insts, b->d_tile_inst, B);
     CK(cudaGetLastError());
     return SS_OK;
   }

@@ -114,7 +114,7 @@ __host__ __device__ constexpr size_t tile_buf_bytes() {
 }
 
 // number of staged buffers a mode needs (phi, then velocity, then l)
-__host__ __device__ inline int flow_buffers(int mode) {
+__host__ __device__ constexpr int flow_buffers(int mode) {
   return mode == M_S2 ? 2 : (mode == M_S3 || mode == M_S4 || mode == M_S23) ? 3 : 1;
 }
 
