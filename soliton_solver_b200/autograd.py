@@ -7,9 +7,18 @@ projection and with the demag psi row as the true dE/dpsi (ss_energy_gradient).
 It agrees with the derivative of the discrete sum up to O(h^4) interior terms and
 the masked boundary ring; ``tests/test_autograd.py`` states the tolerance.
 
-The native calls are registered as torch.library custom ops
-(``soliton_b200::energy`` and ``soliton_b200::energy_gradient``) so they compose
-with torch's dispatcher; solvers are passed by an integer key of ``register()``.
+The native calls are registered as torch.library custom ops so they compose with
+torch's dispatcher (fake tensors, opcheck); solvers are passed by an integer key of
+``register()``:
+
+  soliton_b200::energy(field, key) -> f64 scalar          ss_energy (differentiable)
+  soliton_b200::energy_gradient(field, key) -> like field  ss_energy_gradient
+  soliton_b200::gradient(field, key) -> like field         ss_gradient (projected EG)
+  soliton_b200::charge(field, key, which) -> f64 scalar    ss_charge
+  soliton_b200::coupling_grad(field, key, name) -> f64     ss_coupling_grad
+  soliton_b200::flow_step(field!, velocity!, key, n_steps, prev_energy) -> (E, err)
+                                                           ss_step_async on field and
+                                                           velocity (mutated in place)
 
 ``coupling_gradients(sim, names)`` returns dE/dc at the current field for the
 couplings of the theory (kappa, mpi for the baby Skyrme model, Lambda for
@@ -56,6 +65,62 @@ def energy_gradient_op(field: torch.Tensor, key: int) -> torch.Tensor:
 @energy_gradient_op.register_fake
 def _(field, key):
     return torch.empty_like(field)
+
+
+@torch.library.custom_op("soliton_b200::gradient", mutates_args=())
+def gradient_op(field: torch.Tensor, key: int) -> torch.Tensor:
+    s = _SOLVERS[key]
+    out = torch.empty_like(field)
+    s.gradient(field.contiguous(), out, None)
+    return out
+
+
+@gradient_op.register_fake
+def _(field, key):
+    return torch.empty_like(field)
+
+
+@torch.library.custom_op("soliton_b200::charge", mutates_args=())
+def charge_op(field: torch.Tensor, key: int, which: str) -> torch.Tensor:
+    s = _SOLVERS[key]
+    return torch.tensor(s.charge(field.contiguous(), which), dtype=torch.float64, device=field.device)
+
+
+@charge_op.register_fake
+def _(field, key, which):
+    return field.new_empty((), dtype=torch.float64)
+
+
+@torch.library.custom_op("soliton_b200::coupling_grad", mutates_args=())
+def coupling_grad_op(field: torch.Tensor, key: int, name: str) -> torch.Tensor:
+    s = _SOLVERS[key]
+    return torch.tensor(s.coupling_grad(field.contiguous(), name), dtype=torch.float64, device=field.device)
+
+
+@coupling_grad_op.register_fake
+def _(field, key, name):
+    return field.new_empty((), dtype=torch.float64)
+
+
+@torch.library.custom_op("soliton_b200::flow_step", mutates_args=("field", "velocity"))
+def flow_step_op(field: torch.Tensor, velocity: torch.Tensor, key: int, n_steps: int,
+                 prev_energy: float) -> tuple[torch.Tensor, torch.Tensor]:
+    """n_steps arrested-Newton-flow steps of `field` and `velocity` in place; energy and
+    err trajectories stay on the device (no host synchronisation).  Buffers other than
+    the solver's bound ones are bound first (which starts a fresh arrest history, as
+    Solver.bind does)."""
+    s = _SOLVERS[key]
+    if s.field is None or field.data_ptr() != s.field.data_ptr() or velocity.data_ptr() != s.velocity.data_ptr():
+        s.bind(field, velocity)
+    E = torch.empty(n_steps, dtype=torch.float64, device=field.device)
+    err = torch.empty(n_steps, dtype=torch.float64, device=field.device)
+    s.step_async(n_steps, prev_energy, E, err)
+    return E, err
+
+
+@flow_step_op.register_fake
+def _(field, velocity, key, n_steps, prev_energy):
+    return (field.new_empty((n_steps,), dtype=torch.float64), field.new_empty((n_steps,), dtype=torch.float64))
 
 
 def _setup(ctx, inputs, output):

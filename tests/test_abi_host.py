@@ -98,3 +98,23 @@ def test_render_rgba_validates_arguments_on_the_host():
     assert lib.ss_render_rgba(nat.SS_RENDER_GRAY, buf, nat.SS_FP32, 4, 4, 0.0, 1.0, ctypes.c_void_p(66), None) \
         == nat.SS_ERR_ARG
     assert b"aligned" in lib.ss_last_error()
+
+
+def test_custom_ops_registered_with_fake_shapes():
+    """The torch.library ops exist without a GPU, and their fake implementations give
+    the output shapes and dtypes (what torch.compile and fake-tensor tracing see)."""
+    import torch
+    from torch._subclasses.fake_tensor import FakeTensorMode
+
+    from soliton_solver_b200 import autograd as ops  # noqa: F401 (registers the ops)
+    for name in ("energy", "energy_gradient", "gradient", "charge", "coupling_grad", "flow_step"):
+        assert hasattr(torch.ops.soliton_b200, name)
+    with FakeTensorMode():
+        f = torch.empty(4 * 8 * 8, dtype=torch.float32)
+        v = torch.empty_like(f)
+        g = torch.ops.soliton_b200.gradient(f, 1)
+        assert g.shape == f.shape and g.dtype == f.dtype
+        q = torch.ops.soliton_b200.charge(f, 1, "skyrmion")
+        assert q.shape == () and q.dtype == torch.float64
+        E, err = torch.ops.soliton_b200.flow_step(f, v, 1, 7, 0.0)
+        assert E.shape == (7,) and err.shape == (7,) and E.dtype == torch.float64
