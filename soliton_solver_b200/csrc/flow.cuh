@@ -817,7 +817,7 @@ __host__ __device__ constexpr size_t pipe_slot_bytes() {
 // are per CTA.
 template <class TH, int MODE>
 __host__ __device__ constexpr int pipe_ctas() {
-  return ((MODE == M_S1 || MODE == M_ENERGY) && TH::PAIR_ENERGY) ? 4 : 1;
+  return (MODE == M_S1 || MODE == M_ENERGY) ? TH::S1_CTAS : 1;
 }
 template <class TH, int MODE>
 __host__ __device__ constexpr int pipe_threads() {

@@ -10,6 +10,9 @@
 //   energy()         energy density (FP64), already multiplied by dA
 //   PAIR_ENERGY      energy_pair<V>() exists: the energy point (without dA) of a packed
 //                    FP32 site pair, used for the flow's per-step energy in stage 1
+//   S1_CTAS          resident CTAs per SM of the pipelined stage 1 and energy pass: 4
+//                    (256 threads, 64 registers) for the light chiral stencil, else 1
+//                    (512 threads)
 // plus the charge densities / coupling partials it supports.  Every function
 // states the reference lines it restates.
 #pragma once
@@ -45,6 +48,7 @@ __device__ inline double skyrmion_density(const Jet1<double, NF>& J, double dA) 
 struct ChiralMagnet {
   static constexpr int NF = 4, NMAG = 3;
   static constexpr bool CONSTRAINED = true, HALO_ZERO = true, NEED_XY = false, PAIR_ENERGY = true;
+  static constexpr int S1_CTAS = 4;
 
   // do_gradient_step_point, kernels.py:398-503 (halo zeroing and projection are
   // applied by the caller, kernels.py:505-511).  Constants are pre-scaled so every
@@ -178,7 +182,8 @@ struct ChiralMagnet {
 // ===========================================================================
 struct BabySkyrme {
   static constexpr int NF = 3, NMAG = 3;
-  static constexpr bool CONSTRAINED = true, HALO_ZERO = false, NEED_XY = true, PAIR_ENERGY = false;
+  static constexpr bool CONSTRAINED = true, HALO_ZERO = false, NEED_XY = true, PAIR_ENERGY = true;
+  static constexpr int S1_CTAS = 1;
   template <typename R>
   __device__ static inline void true_rows(R*, const Phys&) {}
 
@@ -335,6 +340,48 @@ struct BabySkyrme {
     return e * dA;
   }
 
+  // the same energy point for a packed FP32 site pair, without dA (the flow's per-step
+  // energy from the gradient's jets; FP32 rounding per site, FP64 sums)
+  template <typename V>
+  __device__ static inline V energy_pair(const Jet<V, NF>& J, const Phys& P) {
+    const V mpi2(P.cf[0] * P.cf[0]), hk2(0.5f * (P.cf[1] * P.cf[1])), half(0.5f), one(1.0f);
+    V g = J.dx[0] * J.dx[0];
+    g = vfma(J.dx[1], J.dx[1], g);
+    g = vfma(J.dx[2], J.dx[2], g);
+    g = vfma(J.dy[0], J.dy[0], g);
+    g = vfma(J.dy[1], J.dy[1], g);
+    g = vfma(J.dy[2], J.dy[2], g);
+    V e = half * g;
+    const V cx = vfma(J.dx[1], J.dy[2], -(J.dx[2] * J.dy[1]));
+    const V cy = vfma(J.dx[2], J.dy[0], -(J.dx[0] * J.dy[2]));
+    const V cz = vfma(J.dx[0], J.dy[1], -(J.dx[1] * J.dy[0]));
+    e = vfma(hk2, vfma(cx, cx, vfma(cy, cy, cz * cz)), e);
+    const V m1 = J.f[0], m2 = J.f[1], m3 = J.f[2];
+    const V t = one - m3;
+    V u(0.0f);
+    if (P.k[0]) u = u + t;
+    if (P.k[1]) u = vfma(t * t, t * t, u);
+    if (P.k[2]) u = vfma(half * m1, m1, u);
+    if (P.k[3]) u = vfma(half * vfma(-m1, m1, one), vfma(-m3, m3, one), u);
+    if (P.k[4]) u = vfma(half * t, vfma(t * t, t, one), u);
+    if (P.k[5]) {
+      const V q = vfma(V(3.0f) * m1, m2 * m2, vfma(V(3.0f) * m3, m3, one)) - m1 * m1 * m1;
+      u = vfma(V(16.0f) * t, q, u);
+    }
+    if (P.k[6]) {
+      V zr = m1, zi = m2;
+      for (int i = 0; i < P.k[8] - 1; ++i) {
+        const V tr = vfma(zr, m1, -(zi * m2));
+        zi = vfma(zr, m2, zi * m1);
+        zr = tr;
+      }
+      const V wr = one - zr;
+      u = vfma(t, vfma(wr, wr, zi * zi), u);
+    }
+    if (P.k[7]) u = u + vfma(-m3, m3, one);
+    return vfma(mpi2, u, e);
+  }
+
   __device__ static inline double charge(const Jet1<double, NF>& J, const Phys&, int, double dA) {
     return skyrmion_density<NF>(J, dA);
   }
@@ -361,6 +408,7 @@ struct BabySkyrme {
 struct GinzburgLandau {
   static constexpr int NF = 4, NMAG = 0;
   static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true, PAIR_ENERGY = false;
+  static constexpr int S1_CTAS = 1;
   template <typename R>
   __device__ static inline void true_rows(R*, const Phys&) {}
 
@@ -430,6 +478,7 @@ struct GinzburgLandau {
 struct Anisotropic {
   static constexpr int NF = 6, NMAG = 0;
   static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true, PAIR_ENERGY = false;
+  static constexpr int S1_CTAS = 1;
   template <typename R>
   __device__ static inline void true_rows(R*, const Phys&) {}
 
