@@ -407,7 +407,7 @@ struct BabySkyrme {
 // ===========================================================================
 struct GinzburgLandau {
   static constexpr int NF = 4, NMAG = 0;
-  static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true, PAIR_ENERGY = false;
+  static constexpr bool CONSTRAINED = false, HALO_ZERO = false, NEED_XY = true, PAIR_ENERGY = true;
   static constexpr int S1_CTAS = 1;
   template <typename R>
   __device__ static inline void true_rows(R*, const Phys&) {}
@@ -451,6 +451,30 @@ struct GinzburgLandau {
     const double curlA = J.dx[1] - J.dy[0];
     e += 0.5 * curlA * curlA;
     return e * dA;
+  }
+
+  // the same energy point for a packed FP32 site pair, without dA (flow energies from
+  // the gradient's jets, FP64 sums); u as above
+  template <typename V>
+  __device__ static inline V energy_pair(const Jet<V, NF>& J, const Phys& P) {
+    const float qf = P.cf[0], uf = P.cf[3];
+    const V q(qf), hq2(0.5f * (qf * qf)), lam8(0.125f * P.cf[1]), u2(uf * uf), half(0.5f);
+    const V A1 = J.f[0], A2 = J.f[1], p1 = J.f[2], p2 = J.f[3];
+    const V p1x = J.dx[2], p1y = J.dy[2], p2x = J.dx[3], p2y = J.dy[3];
+    const V psq = vfma(p1, p1, p2 * p2);
+    const V Asq = vfma(A1, A1, A2 * A2);
+    V g = p1x * p1x;
+    g = vfma(p1y, p1y, g);
+    g = vfma(p2x, p2x, g);
+    g = vfma(p2y, p2y, g);
+    V e = half * g;
+    e = vfma(q * A1, vfma(p1, p2x, -(p2 * p1x)), e);
+    e = vfma(q * A2, vfma(p1, p2y, -(p2 * p1y)), e);
+    e = vfma(hq2 * Asq, psq, e);
+    const V d = u2 - psq;
+    e = vfma(lam8 * d, d, e);
+    const V curl = J.dx[1] - J.dy[0];
+    return vfma(half * curl, curl, e);
   }
 
   // compute_vortex_density, kernels.py:146-178
