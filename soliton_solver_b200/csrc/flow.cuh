@@ -90,12 +90,37 @@ struct TileShape {
 };
 
 // Centre of a tile (TX x TY sites, NF components) of phi and V into A.copy_phi /
-// A.copy_vel, from the staged halo tiles Pt / Vt (phi and V as loaded) or, when those
-// are null, from A.phi / A.vel.  Rows of TY consecutive values: coalesced stores.
+// A.copy_vel (each skipped when null), from the staged halo tiles Pt / Vt (phi and V
+// as loaded) or, when those are null, from A.phi / A.vel.  Lattice rows whose length
+// is a multiple of 16 bytes (always so under TMA staging) copy 16-byte vectors: staged
+// rows start 16-byte aligned (the pitch and the y offset are multiples of 16 bytes).
 template <int NF, typename R, int TX, int TY, int NT, typename FA>
 __device__ __forceinline__ void copy_centre(const FA& A, const R* Pt, const R* Vt, int x0, int y0) {
   using TS = TileShape<TX, TY, NT>;
   const Grid& G = A.G;
+  constexpr int VW = 16 / sizeof(R);  // elements per 16-byte vector
+  static_assert(TY % VW == 0 && (TS::HY * sizeof(R)) % 16 == 0 && (TS::YOFF * sizeof(R)) % 16 == 0, "alignment");
+  auto al16 = [](const void* q) { return ((uintptr_t)q & 15u) == 0; };  // null counts as aligned
+  // rows of whole vectors, and every base pointer involved 16-byte aligned (the caller's
+  // buffers need not be under plain staging); uniform over the block
+  const bool vec = G.Y % VW == 0 && al16(A.copy_phi) && al16(A.copy_vel) && (Pt || !A.copy_phi || al16(A.phi)) &&
+                   (Vt || !A.copy_vel || al16(A.vel));
+  if (vec) {
+    constexpr int RV = TY / VW;  // vectors per tile row
+#pragma unroll 2
+    for (int i = threadIdx.x; i < NF * TX * RV; i += NT) {
+      const int yv = i % RV, lx = (i / RV) % TX, a = i / (TX * RV);
+      const int gx = x0 + lx, gy = y0 + yv * VW;
+      if (gx >= G.X || gy >= G.Y) continue;
+      const long long g = a * G.N + (long long)gx * G.Y + gy;
+      const int t = a * TS::PLANE + (lx + 2) * TS::HY + TS::YOFF + yv * VW;
+      if (A.copy_phi)
+        *reinterpret_cast<uint4*>(A.copy_phi + g) = *reinterpret_cast<const uint4*>(Pt ? Pt + t : A.phi + g);
+      if (A.copy_vel)
+        *reinterpret_cast<uint4*>(A.copy_vel + g) = *reinterpret_cast<const uint4*>(Vt ? Vt + t : A.vel + g);
+    }
+    return;
+  }
 #pragma unroll 4
   for (int i = threadIdx.x; i < NF * TX * TY; i += NT) {
     const int y = i % TY, lx = (i / TY) % TX, a = i / (TX * TY);
@@ -103,8 +128,8 @@ __device__ __forceinline__ void copy_centre(const FA& A, const R* Pt, const R* V
     if (gx >= G.X || gy >= G.Y) continue;
     const long long g = a * G.N + (long long)gx * G.Y + gy;
     const int t = a * TS::PLANE + (lx + 2) * TS::HY + TS::YOFF + y;
-    A.copy_phi[g] = Pt ? Pt[t] : A.phi[g];
-    A.copy_vel[g] = Vt ? Vt[t] : A.vel[g];
+    if (A.copy_phi) A.copy_phi[g] = Pt ? Pt[t] : A.phi[g];
+    if (A.copy_vel) A.copy_vel[g] = Vt ? Vt[t] : A.vel[g];
   }
 }
 
@@ -635,7 +660,7 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
       return;
     }
     if constexpr (mode == M_S2 || mode == M_S23) {
-      if (A.copy_phi) {  // uniform over the block
+      if (A.copy_phi || A.copy_vel) {  // uniform over the block
         copy_centre<NF, R, TX, TY, NT>(A, B0, B1, x0, y0);
         __syncthreads();  // every value is copied before the combine overwrites V in place
       }
@@ -686,7 +711,7 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
     if constexpr (uses_v) arrest = st->arrest != 0;
     stage_plain<NF, R, TX, TY, NT>(B0, A, x0, y0, mode, arrest);
     if constexpr (mode == M_S2) {
-      if (A.copy_phi) copy_centre<NF, R, TX, TY, NT>(A, (const R*)nullptr, (const R*)nullptr, x0, y0);
+      if (A.copy_phi || A.copy_vel) copy_centre<NF, R, TX, TY, NT>(A, (const R*)nullptr, (const R*)nullptr, x0, y0);
     }
     __syncthreads();
   }
