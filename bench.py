@@ -22,6 +22,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -72,7 +73,9 @@ class Clocks:
         self.index = index
         self.proc = None
         self.marks = []
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{index}.csv")
+        # raw samples: SS_BENCH_CLOCKS_DIR when set (to keep them), else the temp directory
+        out = os.environ.get("SS_BENCH_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out, f"clocks_gpu{index}.csv")
 
     def __enter__(self):
         try:
