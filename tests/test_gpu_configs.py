@@ -84,20 +84,29 @@ def test_c3_lambda_adjoint_four_vortices(lam, steps, tol):
     assert abs(g - fd) <= tol * abs(fd), (g, fd)
 
 
-@pytest.mark.parametrize("demag", [False, True])
-def test_chiral_coupling_adjoints_relaxed(demag):
+@pytest.mark.parametrize("demag,steps,warm", [(False, 150000, 40000), (True, 250000, 60000)])
+def test_chiral_coupling_adjoints_relaxed(demag, steps, warm):
+    """dE_min/dB, dK, dD from the coupling kernel at the relaxed anti-skyrmion against central
+    differences (dc = 1e-2 c) of relaxed energies, to 1e-4.
+
+    The flow relaxes to the zero of the reference's 4th-order stencil gradient, which differs
+    from the derivative of the discrete energy sum by O(h^4); the envelope theorem then holds to
+    that order.  Measured for B without demag: 4.1e-2, 2.6e-3, 1.6e-4 at h = 0.125, 0.063, 0.031
+    (box size irrelevant), so the check runs at h = 10/511 = 0.0196 (measured <= 6.2e-5).  The
+    shifted relaxations start from the relaxed field."""
     th = load_theory("Chiral magnet")
-    kw = dict(xlen=256, ylen=256, xsize=16.0, ysize=16.0, J=40e-12, K=0.8e6, D=4e-3, M=580e3, B=0.2,
+    kw = dict(xlen=512, ylen=512, xsize=10.0, ysize=10.0, J=40e-12, K=0.8e6, D=4e-3, M=580e3, B=0.2,
               dmi_term="Heusler", demag=demag, unit_magnetization=True)
     field = lambda rp: anti_skyrmion(rp, R=1.0, seed=0, device="cuda")  # noqa: E731
-    steps = 30000
     sim, _ = _relaxed(th, kw, field, steps)
     g = coupling_gradients(sim)
-    assert abs(sim.observables()["skyrmion_number"] - 1.0) < 1e-3
+    assert abs(sim.observables()["skyrmion_number"] - 1.0) < 1e-4
+    F = sim.Field.clone()
+    relaxed_from = lambda rp: F  # noqa: E731
     for name in ("B", "K", "D"):
         c = kw[name]
-        d = 1e-3 * c
-        _, Ep = _relaxed(th, dict(kw, **{name: c + d}), field, steps)
-        _, Em = _relaxed(th, dict(kw, **{name: c - d}), field, steps)
+        d = 1e-2 * c
+        _, Ep = _relaxed(th, dict(kw, **{name: c + d}), relaxed_from, warm)
+        _, Em = _relaxed(th, dict(kw, **{name: c - d}), relaxed_from, warm)
         fd = (Ep - Em) / (2 * d)
-        assert abs(g[name] - fd) <= 2e-2 * abs(fd), (name, g[name], fd)
+        assert abs(g[name] - fd) <= 1e-4 * abs(fd), (name, g[name], fd)
