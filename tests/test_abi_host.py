@@ -28,6 +28,14 @@ def test_library_exports_every_declared_symbol():
     assert lib.ss_abi_version() == 1
 
 
+def test_integration_guide_lists_every_entry_point():
+    """Every entry point the header declares has a row (or a mention) in the integration
+    guide, which says which reference interface it replaces."""
+    guide = open(os.path.join(os.path.dirname(HEADER), os.pardir, "INTEGRATION.md")).read()
+    missing = [n for n in _declared() if n not in guide]
+    assert not missing, missing
+
+
 def _create(theory_name, **kw):
     th = load_theory(theory_name)
     p_i, p_f = th.params.pack_device_params(th.params.default_params(**kw).resolved())
