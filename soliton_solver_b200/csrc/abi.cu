@@ -1430,8 +1430,15 @@ struct ss_batch {
   std::vector<void*> fields, vels;
   long long wait_cycles = WAIT_CYCLES;
   cudaGraphExec_t graph = nullptr;
+  // per-lattice step states and trajectory rows, contiguous in the workspace (lattice i:
+  // d_st[i], d_E / d_err rows i * TRAJ_CAP), so that one copy returns each for all lattices
+  StepState* d_st = nullptr;
+  double* d_E = nullptr;
+  double* d_err = nullptr;
+  char* h_stage = nullptr;  // page-locked staging of those copies (first ss_batch_step)
   ~ss_batch() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (h_stage) cudaFreeHost(h_stage);
   }
 };
 
@@ -1447,14 +1454,17 @@ size_t batch_layout(ss_batch* b, char* base) {
   b->d_insts = (BatchInst*)take(sizeof(BatchInst) * b->n);
   b->d_tile_inst = (int*)take(sizeof(int) * b->total_tiles);
   b->d_prev = (double*)take(sizeof(double) * b->n);
+  b->d_st = (StepState*)take(sizeof(StepState) * b->n);
+  b->d_E = (double*)take(sizeof(double) * TRAJ_CAP * b->n);
+  b->d_err = (double*)take(sizeof(double) * TRAJ_CAP * b->n);
   b->h_insts.assign(b->n, BatchInst{});
   for (int i = 0; i < b->n; ++i) {
     BatchInst& I = b->h_insts[i];
     const size_t fb = b->elem * (size_t)b->nf * (size_t)b->inst[i].G.N;
-    I.st = (StepState*)take(sizeof(StepState));
+    I.st = b->d_st ? b->d_st + i : nullptr;
     I.partial = (double*)take(sizeof(double) * b->tiles[i]);
-    I.E_traj = (double*)take(sizeof(double) * TRAJ_CAP);
-    I.err_traj = (double*)take(sizeof(double) * TRAJ_CAP);
+    I.E_traj = b->d_E ? b->d_E + (size_t)i * TRAJ_CAP : nullptr;
+    I.err_traj = b->d_err ? b->d_err + (size_t)i * TRAJ_CAP : nullptr;
     for (int k = 2; k < 7; ++k) I.buf[k] = take(fb);
   }
   return off;
@@ -1586,7 +1596,8 @@ int ss_batch_destroy(ss_batch* b) {
 int ss_batch_workspace_bytes(const ss_batch* b, size_t* bytes) {
   if (!b || !bytes) return fail(SS_ERR_ARG, "NULL argument");
   ss_batch tmp = *b;
-  tmp.graph = nullptr;  // the copy must not own the original's graph
+  tmp.graph = nullptr;  // the copy must not own the original's graph or staging
+  tmp.h_stage = nullptr;
   *bytes = batch_layout(&tmp, nullptr);
   return SS_OK;
 }
@@ -1623,8 +1634,8 @@ int ss_batch_bind(ss_batch* b, void* const* fields, void* const* velocities, voi
   StepState init;
   memset(&init, 0, sizeof(init));
   init.E_last = NAN;
-  for (int i = 0; i < b->n; ++i)
-    CK(cudaMemcpyAsync(b->h_insts[i].st, &init, sizeof(init), cudaMemcpyHostToDevice, b->stream));
+  const std::vector<StepState> inits(b->n, init);  // pageable: staged before the call returns
+  CK(cudaMemcpyAsync(b->d_st, inits.data(), sizeof(StepState) * b->n, cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->d_insts, b->h_insts.data(), sizeof(BatchInst) * b->n, cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->d_tile_inst, tile_inst.data(), sizeof(int) * b->total_tiles, cudaMemcpyHostToDevice,
                      b->stream));
@@ -1638,6 +1649,15 @@ int ss_batch_step(ss_batch* b, int n_steps, const double* prev_energy, double* e
   if (prev_energy)
     CK(cudaMemcpyAsync(b->d_prev, prev_energy, sizeof(double) * b->n, cudaMemcpyHostToDevice, b->stream));
   bool use_prev = prev_energy != nullptr;
+  // trajectories (k columns of every lattice's row) and the step states come back through
+  // page-locked staging: one 2-D copy each, one synchronisation per chunk
+  const size_t nn = (size_t)b->n;
+  if (!b->h_stage)
+    CK(cudaHostAlloc((void**)&b->h_stage, 2 * nn * TRAJ_CAP * sizeof(double) + nn * sizeof(StepState),
+                     cudaHostAllocDefault));
+  double* hE = reinterpret_cast<double*>(b->h_stage);
+  double* hErr = hE + nn * TRAJ_CAP;
+  StepState* hst = reinterpret_cast<StepState*>(hErr + nn * TRAJ_CAP);
   for (int done = 0; done < n_steps; done += TRAJ_CAP) {
     const int k = std::min(TRAJ_CAP, n_steps - done);
     int rc = batch_dispatch(b, [&](auto* tag) -> int {
@@ -1647,24 +1667,23 @@ int ss_batch_step(ss_batch* b, int n_steps, const double* prev_energy, double* e
     });
     if (rc) return rc;
     use_prev = false;
-    for (int i = 0; i < b->n; ++i) {
-      if (energy_traj)
-        CK(cudaMemcpyAsync(energy_traj + (size_t)i * n_steps + done, b->h_insts[i].E_traj, k * sizeof(double),
-                           cudaMemcpyDeviceToHost, b->stream));
-      if (err_traj)
-        CK(cudaMemcpyAsync(err_traj + (size_t)i * n_steps + done, b->h_insts[i].err_traj, k * sizeof(double),
-                           cudaMemcpyDeviceToHost, b->stream));
+    const size_t row = k * sizeof(double), pitch = TRAJ_CAP * sizeof(double);
+    if (energy_traj) CK(cudaMemcpy2DAsync(hE, row, b->d_E, pitch, row, nn, cudaMemcpyDeviceToHost, b->stream));
+    if (err_traj) CK(cudaMemcpy2DAsync(hErr, row, b->d_err, pitch, row, nn, cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    for (size_t i = 0; i < nn; ++i) {
+      if (energy_traj) memcpy(energy_traj + i * n_steps + done, hE + i * k, row);
+      if (err_traj) memcpy(err_traj + i * n_steps + done, hErr + i * k, row);
     }
   }
+  CK(cudaMemcpyAsync(hst, b->d_st, nn * sizeof(StepState), cudaMemcpyDeviceToHost, b->stream));
   CK(cudaStreamSynchronize(b->stream));
   int worst = 0;
-  for (int i = 0; i < b->n; ++i) {
-    StepState st;
-    CK(cudaMemcpy(&st, b->h_insts[i].st, sizeof(st), cudaMemcpyDeviceToHost));
-    if (st.status) {
-      worst = st.status;
+  for (size_t i = 0; i < nn; ++i) {
+    if (hst[i].status) {
+      worst = hst[i].status;
       const int zero = 0;
-      CK(cudaMemcpy(&b->h_insts[i].st->status, &zero, sizeof(int), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(&b->d_st[i].status, &zero, sizeof(int), cudaMemcpyHostToDevice));
     }
   }
   if (worst == SS_ERR_TIMEOUT) return fail(SS_ERR_TIMEOUT, "a device-side wait timed out; re-bind the batch");
@@ -1751,14 +1770,11 @@ int ss_batch_graph_launch(ss_batch* b) {
 int ss_batch_trajectory(ss_batch* b, int n_steps, double* energy_traj, double* err_traj) {
   if (!b || !b->ws) return fail(SS_ERR_STATE, "batch not bound");
   if (n_steps < 0 || n_steps > TRAJ_CAP) return fail(SS_ERR_ARG, "n_steps must be in 0..%d", TRAJ_CAP);
-  for (int i = 0; i < b->n; ++i) {
-    if (energy_traj)
-      CK(cudaMemcpyAsync(energy_traj + (size_t)i * n_steps, b->h_insts[i].E_traj, n_steps * sizeof(double),
-                         cudaMemcpyDeviceToHost, b->stream));
-    if (err_traj)
-      CK(cudaMemcpyAsync(err_traj + (size_t)i * n_steps, b->h_insts[i].err_traj, n_steps * sizeof(double),
-                         cudaMemcpyDeviceToHost, b->stream));
-  }
+  const size_t row = n_steps * sizeof(double), pitch = TRAJ_CAP * sizeof(double);
+  if (n_steps > 0 && energy_traj)
+    CK(cudaMemcpy2DAsync(energy_traj, row, b->d_E, pitch, row, b->n, cudaMemcpyDeviceToHost, b->stream));
+  if (n_steps > 0 && err_traj)
+    CK(cudaMemcpy2DAsync(err_traj, row, b->d_err, pitch, row, b->n, cudaMemcpyDeviceToHost, b->stream));
   CK(cudaStreamSynchronize(b->stream));
   return SS_OK;
 }
