@@ -283,7 +283,8 @@ int ss_batch_bind(ss_batch *b, void *const *fields, void *const *velocities, voi
                   size_t workspace_bytes, void *stream);
 /* n_steps steps of every lattice.  prev_energy (host, n_lattices, nullable: continue
  * from the device state) seeds each first arrest test; energy_traj / err_traj (host,
- * nullable) receive lattice-major [i * n_steps + s] trajectories. */
+ * nullable) receive lattice-major [i * n_steps + s] trajectories.  The first call
+ * page-locks a host staging buffer of 16 KB per lattice, held until ss_batch_destroy. */
 int ss_batch_step(ss_batch *b, int n_steps, const double *prev_energy, double *energy_traj, double *err_traj);
 int ss_batch_tma_enabled(const ss_batch *b);
 
