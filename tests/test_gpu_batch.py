@@ -66,8 +66,9 @@ def test_batch_matches_single_lattices(precision, aligned):
     assert np.all(np.isfinite(E2))
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
 @pytest.mark.parametrize("aligned", [True, False], ids=["tma", "plain"])
-def test_batch_odd_step_counts_are_bitwise_invariant(aligned):
+def test_batch_odd_step_counts_are_bitwise_invariant(aligned, precision):
     """The last step of an odd-count batched call ends in the caller's buffers (stage 2
     copies phi and V into the alternates, stage 4 runs at the opposite parity): seven
     steps split into odd and even calls equal one call bitwise, arrests included."""
@@ -82,8 +83,9 @@ def test_batch_odd_step_counts_are_bitwise_invariant(aligned):
     prev[0] = -1e300  # arrest fires for this lattice
     outs = []
     for split in ([7], [1, 2, 1, 3], [3, 3, 1]):
-        b = BatchSolver(th, params, "fp32")
-        assert b.tma_enabled == aligned
+        b = BatchSolver(th, params, precision)
+        es = 4 if precision == "fp32" else 8
+        assert b.tma_enabled == all(Y * es % 16 == 0 for _, Y in sizes)
         for i, F in enumerate(fields):
             b.load(i, F)
         Es = []
@@ -98,6 +100,35 @@ def test_batch_odd_step_counts_are_bitwise_invariant(aligned):
             np.testing.assert_array_equal(a, c)
         for a, c in zip(vs, outs[0][2]):
             np.testing.assert_array_equal(a, c)
+
+
+def test_batch_trajectories_across_chunks():
+    """A call longer than the 1024-step trajectory chunk: every lattice's energy and err
+    rows (returned per chunk in one 2-D copy for all lattices) equal a single-lattice
+    solver's, and the fields end equal."""
+    th = load_theory("Baby Skyrme")
+    sizes = [(24, 32), (40, 36), (33, 20)]
+    rng = np.random.default_rng(3)
+    params = [th.params.default_params(xlen=X, ylen=Y, lsx=0.1, lsy=0.1, time_step=0.02,
+                                       kappa=float(rng.uniform(0.5, 2)), mpi=float(rng.uniform(0.5, 2)),
+                                       unit_magnetization=True) for X, Y in sizes]
+    fields = [_hedgehog(p.resolved(), B=1 + i, R=1.5, seed=i) for i, p in enumerate(params)]
+    b = BatchSolver(th, params, "fp64")
+    for i, F in enumerate(fields):
+        b.load(i, F)
+    n = 1030
+    E, err = b.step(n, np.full(len(sizes), 1e300))
+    assert E.shape == (len(sizes), n) and np.isfinite(E).all()
+    for i, p in enumerate(params):
+        p_i, p_f = th.params.pack_device_params(p.resolved())
+        s = Solver(th.kernels.THEORY_ID, p_i, p_f, "fp64")
+        f = torch.tensor(fields[i].reshape(-1), dtype=torch.float64, device="cuda")
+        v = torch.zeros_like(f)
+        s.bind(f, v)
+        Ei, erri = s.step(n, 1e300)
+        np.testing.assert_allclose(E[i], Ei, rtol=1e-12)
+        np.testing.assert_allclose(err[i], erri, rtol=1e-10, atol=1e-300)
+        np.testing.assert_allclose(b.fields[i].cpu().numpy(), f.cpu().numpy(), rtol=0, atol=1e-11)
 
 
 def test_batch_sweep_config_shape():
