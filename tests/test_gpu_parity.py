@@ -259,6 +259,31 @@ def test_step_chunking_is_bitwise_invariant():
         np.testing.assert_array_equal(v, outs[0][2])
 
 
+def test_step_across_trajectory_chunks_equals_one_async_call():
+    """ss_step runs 1024-step chunks (trajectories and device state back through page-locked
+    staging after each); 1030 steps that way equal one ss_step_async call bitwise."""
+    theory = load_theory("Chiral magnet")
+    rp = theory.params.default_params(xlen=64, ylen=96, xsize=4.0, ysize=6.0, dmi_term="Heusler", demag=True,
+                                      unit_magnetization=True).resolved()
+    p_i, p_f = theory.params.pack_device_params(rp)
+    F = _smooth_field("chiral_magnet", rp, 13)
+    n = 1030
+    a = Solver(0, p_i, p_f, "fp32")
+    fa, va = _dev(F, "fp32"), _dev(np.zeros_like(F), "fp32")
+    a.bind(fa, va)
+    E, err = a.step(n, 1e300)
+    b = Solver(0, p_i, p_f, "fp32")
+    fb, vb = _dev(F, "fp32"), _dev(np.zeros_like(F), "fp32")
+    b.bind(fb, vb)
+    Ed = torch.empty(n, dtype=torch.float64, device="cuda")
+    errd = torch.empty(n, dtype=torch.float64, device="cuda")
+    b.step_async(n, 1e300, Ed, errd)
+    b.check_status()
+    np.testing.assert_array_equal(E, Ed.cpu().numpy())
+    np.testing.assert_array_equal(err, errd.cpu().numpy())
+    assert torch.equal(fa, fb) and torch.equal(va, vb)
+
+
 @pytest.mark.parametrize("Y", [192, 150], ids=["tma", "plain"])
 def test_odd_step_counts_every_variant(Y):
     """A call with an odd step count ends in the caller's buffers without a copy back:
