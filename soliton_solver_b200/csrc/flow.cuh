@@ -382,9 +382,12 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
   double e_pair = 0.0;
   const int j = threadIdx.x % PAIRS;
   const int lxg = threadIdx.x / PAIRS;
-#pragma unroll 1
+  // stage 1 and the energy pass (which must reduce alike) give each thread adjacent rows;
+  // the energy pass unrolls them so that the rows share their x-neighbour loads
+  constexpr bool ADJ = JE && (MODE == M_S1 || MODE == M_ENERGY);
+#pragma unroll((JE && MODE == M_ENERGY) ? 2 : 1)
   for (int pass = 0; pass < TX / RPP; ++pass) {
-    const int lx = lxg + pass * RPP;
+    const int lx = ADJ ? lxg * (TX / RPP) + pass : lxg + pass * RPP;
     const int gx = x0 + lx, gy = y0 + 2 * j;
     bool v1 = true;
     Masks m0{true, true, true}, m1{true, true, true};
