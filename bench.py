@@ -467,8 +467,18 @@ def render_rgba(dev, F0, reps=20):
     gbs = XLEN * YLEN * 16 / (us * 1e-6) / 1e9
     peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0)) \
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    # beside it: the reference's per-pixel colormap restated on the CPU (the oracle), on a
+    # 128 x 128 corner of the same field
+    from oracle import colormaps as ocm
+    n = 128
+    Fs = F.view(-1, XLEN, YLEN)[:, :n, :n].double().cpu().numpy().reshape(-1)
+    t = time.perf_counter()
+    ocm.render_magnetization(Fs, n, n)
+    cpu_pps = n * n / (time.perf_counter() - t)
     return {"kernel": "render_kernel<float, magnetization> (ss_render_rgba)", "pixels": XLEN * YLEN,
-            "us_per_image": us, "achieved_gbs": gbs, "frac": gbs / peak, "bytes_per_pixel": 16}
+            "us_per_image": us, "achieved_gbs": gbs, "frac": gbs / peak, "bytes_per_pixel": 16,
+            "cpu_pixels_per_s": cpu_pps, "speedup": XLEN * YLEN / (us * 1e-6) / cpu_pps,
+            "cpu_sample": "oracle restatement of the reference's per-pixel colormap, 128x128 corner, 1 core"}
 
 
 def initial_condition(dev, reps=10):
@@ -491,8 +501,17 @@ def initial_condition(dev, reps=10):
     us = e0.elapsed_time(e1) / reps * 1e3
     del sim
     torch.cuda.empty_cache()
+    # beside it: the ansatz restated in numpy on the CPU (the oracle), on a 512^2 lattice
+    from oracle import init as oin
+    thn, pn = chiral_params(512, 512)
+    p_i, p_f = thn.params.pack_device_params(pn.resolved())
+    t = time.perf_counter()
+    oin.initial("chiral_magnet", p_i, p_f, ansatz=oin.ANSATZ_ANTI, rotation=0.3)
+    cpu_sps = 512 * 512 / (time.perf_counter() - t)
     return {"kernel": "init_kernel<chiral, float> (ss_initialize, anti-skyrmion ansatz)", "sites": XLEN * YLEN,
-            "us": us, "achieved_gbs": XLEN * YLEN * 32 / (us * 1e-6) / 1e9, "bytes_per_site": 32}
+            "us": us, "achieved_gbs": XLEN * YLEN * 32 / (us * 1e-6) / 1e9, "bytes_per_site": 32,
+            "cpu_sites_per_s": cpu_sps, "speedup": XLEN * YLEN / (us * 1e-6) / cpu_sps,
+            "cpu_sample": "oracle numpy restatement of the ansatz kernel, 512x512 chiral lattice, 1 process"}
 
 
 def dat_field_dump(dev, F0, reps=3):
