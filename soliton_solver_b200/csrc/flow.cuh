@@ -838,8 +838,8 @@ __host__ __device__ constexpr size_t pipe_slot_bytes() {
          sizeof(R) * NF * TX * TY * pipe_centre_buffers<MODE>();
 }
 
-// Persistent CTAs per SM: four 256-thread CTAs for stage 1 and the energy pass of a
-// theory whose energy point runs in packed FP32 (issue-bound: two site pairs per thread
+// Persistent CTAs per SM: for stage 1 and the energy pass the theory's S1_CTAS (four
+// 256-thread CTAs for the light chiral stencil, issue-bound: two site pairs per thread
 // per tile halve the per-tile overhead, and four CTAs keep 32 warps per SM), one
 // 512-thread CTA otherwise.  Stage 1 and the energy pass must agree: their partials
 // are per CTA.
