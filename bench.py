@@ -162,16 +162,36 @@ def cpu_sample(steps, warmup, threads=None, rows=128):
     return value, threads, sample, dt
 
 
+def reference_sample(steps, warmup, n=16):
+    """The reference's own flow step (baseline/_ref under Numba's CUDA simulator) on
+    independent n x n sub-lattices of the workload, one process per core; falls back
+    to the oracle port when the reference is not installed.  Returns (value, cores,
+    kind, sample, seconds per step)."""
+    sys.path.insert(0, os.path.join(ROOT, "baseline"))
+    import reference_runner as rr
+    why = rr.available()
+    if why is None:
+        value, procs, dt, _ = rr.time_flow_steps(n=n, spacing=XSIZE / (XLEN - 1), steps=steps, warmup=warmup)
+        sample = (f"{procs} independent processes (one core each), each the reference's Simulation.step (FP64 "
+                  f"Numba kernels under NUMBA_ENABLE_CUDASIM=1, soliton_solver 1.1.1 from baseline/_ref) on a "
+                  f"{n}x{n} sub-lattice of the workload (same couplings and spacing, Heusler, demag on, B=0.2 T; "
+                  f"the reference's ground state + N(0,1e-3) noise); {steps} timed steps after {warmup} warm-up")
+        return value, procs, "reference", sample, dt
+    value, threads, sample, dt = cpu_sample(steps, warmup)
+    return value, threads, "port", f"{sample} (reference unavailable: {why})", dt
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return 0
-    steps, warmup = max(args.steps, 1), max(args.warmup, 0)
-    value, threads, sample, dt = cpu_sample(min(steps, 3), min(warmup, 1))
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": min(steps, 3),
-            "warmup": min(warmup, 1), "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+    # each step of the simulator costs ~5 s per 16x16 sample: a bounded number of them
+    steps, warmup = min(max(args.steps, 1), 4), min(max(args.warmup, 0), 1)
+    value, cores, kind, sample, dt = reference_sample(steps, warmup)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": config({"sample": sample}),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -281,10 +301,12 @@ def gpu_arm(args, rank, world, local_rank):
     extra = {}
     if rank == 0 and not args.no_compare:
         extra = compare_fp64_and_plain(args, dev, F0)
-    cpu = None
+    cpu = cpu_port = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, kind, sample, _ = reference_sample(1, 1)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
         v, threads, sample, _ = cpu_sample(1, 0)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        cpu_port = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
                 "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -297,7 +319,7 @@ def gpu_arm(args, rank, world, local_rank):
                                        if fused else "flow_kernel<ChiralMagnet,float> (4 stage launches per step)",
                              "launches_per_step": 3 if fused else 4,
                              "algorithmic_bytes_per_step": bytes_step},
-                "cpu_baseline": cpu,
+                "cpu_baseline": cpu, "cpu_baseline_port": cpu_port,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": Ke, "api": "Simulation.step(prev_energy) per step"},
                 "gpu_launches": launches, "clocks": clk.summary(),

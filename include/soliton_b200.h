@@ -242,18 +242,19 @@ int ss_coupling_grad(ss_handle *h, const void *field, int coupling, double *out)
 
 /* Total energy of `field` (SS_FP32 or SS_FP64 elements, reference layout) with no
  * handle and no allocation of any kind.  No counterpart in the reference: it exists
- * for callers that cannot allocate device memory when they need the energy, e.g.
- * while a stream is being captured into a CUDA graph, inside a host whose memory
- * manager owns the whole device, or in an interactive loop that must not let
- * cudaMalloc synchronise the device.  Its scratch (reduction state and one FP64
+ * for callers that cannot allocate device memory when they need the energy — a host
+ * whose memory manager owns the whole device and forbids further allocations, or an
+ * interactive loop (a viewer's per-frame callback) that must not call cudaMalloc or
+ * cudaFree, which synchronise the device.  Its scratch (reduction state and one FP64
  * partial per 16 x 64-site tile) lives in a 512 KiB static device array that every
  * GPU loading the library holds until exit, so lattices of at most 65504 tiles are
  * accepted (4096 x 4096 needs 16384); larger ones get SS_ERR_ARG.  The first call
- * on a device looks up the array's device address (cudaGetSymbolAddress): make it
- * before any stream capture.  All calls share the array and the kernel runs on
- * `stream` (a cudaStream_t, NULL for the legacy default stream): calls that overlap
- * on the GPU race; each call clears the reduction state before use.  The result is
- * returned in *out after synchronising `stream`. */
+ * on a device looks up the array's device address (cudaGetSymbolAddress, with that
+ * device current): make that first call before any stream capture.  All calls share
+ * the array and the kernel runs on `stream` (a cudaStream_t, NULL for the legacy
+ * default stream): calls that overlap on the GPU race; each call clears the
+ * reduction state before use.  The call synchronises `stream` and returns the
+ * result in *out. */
 int ss_energy_noalloc(int theory, const int32_t *p_i, int n_i, const double *p_f, int n_f, int precision,
                       const void *field, double *out, void *stream);
 

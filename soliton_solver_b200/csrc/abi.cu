@@ -1,5 +1,6 @@
 // abi.cu -- C ABI of libsoliton_b200 (declared in include/soliton_b200.h).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <type_traits>
 #include <cstdarg>
@@ -1329,10 +1330,10 @@ int ss_rk4_finalize(ss_handle* h, void* velocity, void* field, const void* k1, c
 // Total energy without any allocation.
 //
 // Some callers cannot allocate device memory at the point where they need an
-// energy: code that runs while a stream is being captured into a CUDA graph
-// (cudaMalloc is not allowed there), hosts whose memory manager owns the whole
-// device and forbids further allocations, and interactive loops that must not
-// call cudaMalloc because it synchronises the device.  For them
+// energy: hosts whose memory manager owns the whole device and forbids further
+// allocations (a framework's caching allocator or a fixed memory pool), and
+// interactive loops (a viewer's per-frame callback) that must not call cudaMalloc
+// or cudaFree because those synchronise the device and stall the frame.  For them
 // ss_energy_noalloc keeps its scratch (the per-block partial sums and the
 // reduction state) in the file-scope array below, which every GPU that loads
 // this library holds until exit.
@@ -1341,19 +1342,23 @@ namespace {
 
 constexpr size_t NOALLOC_SCRATCH_BYTES = 512 * 1024;   // 256 B state + up to 65504 block partials
 __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
-void* g_noalloc_addr[64] = {};                          // device address of the array, per device
+// Device address of the array, per device.  Host threads calling concurrently on a
+// device that has no entry yet may each look it up; they store the same address, and
+// the atomic (relaxed ordering suffices) makes those concurrent stores well defined.
+std::atomic<void*> g_noalloc_addr[64];
 
-// Device address of the static scratch on the current device (looked up once per device).
+// Device address of the static scratch on the current device (looked up once per device,
+// with that device current: in host code the array's name is only a host-side stand-in).
 int noalloc_scratch(void** out) {
   int dev = -1;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(SS_ERR_ARG, "device ordinal %d out of range", dev);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
+  void* p = g_noalloc_addr[dev].load(std::memory_order_relaxed);
+  if (!p) {
     CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_addr[dev] = p;
+    g_noalloc_addr[dev].store(p, std::memory_order_relaxed);
   }
-  *out = g_noalloc_addr[dev];
+  *out = p;
   return SS_OK;
 }
 

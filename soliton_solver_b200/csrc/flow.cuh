@@ -16,7 +16,9 @@
 // The energy of a step's result is computed by the NEXT step's S1, which stages
 // exactly that field anyway, and the arrest decision is kept on the device
 // (StepState.arrest) and applied by S2..S4 as "V = 0".  A trailing energy pass
-// closes a call.  Compulsory traffic: 16 words per site and step.
+// closes a call.  Compulsory traffic: 16 words per site and step as four kernels
+// (S1 2, S2 3, S3 4, S4 7); 14 when stages 2 and 3 run as one kernel (M_S23), which
+// stages phi, V and l1 once and writes l2 and l3.
 #pragma once
 
 #include <cuda.h>

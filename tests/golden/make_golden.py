@@ -2,7 +2,7 @@
 
 Run in a container that has the reference checkout (it is NOT needed at test time):
 
-    python tests/golden/make_golden.py --ref /root/reference --out tests/golden
+    python tests/golden/make_golden.py --ref <reference checkout> --out tests/golden
 
 It imports the reference package with Numba's CUDA simulator enabled
 (``NUMBA_ENABLE_CUDASIM=1``; no GPU is used) and with empty stand-in modules for
@@ -118,7 +118,8 @@ def _traj_cases():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("SOLITON_SOLVER_REF"), required="SOLITON_SOLVER_REF" not in os.environ,
+                    help="root of the reference soliton_solver checkout (or set SOLITON_SOLVER_REF)")
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
     ap.add_argument("--only", default=None)
     args = ap.parse_args()

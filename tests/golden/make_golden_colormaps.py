@@ -2,7 +2,7 @@
 
 Run in a container that has the reference checkout (it is NOT needed at test time):
 
-    python tests/golden/make_golden_colormaps.py --ref /root/reference --out tests/golden
+    python tests/golden/make_golden_colormaps.py --ref <reference checkout> --out tests/golden
 
 It imports ``soliton_solver.core.colormaps`` with Numba's CUDA simulator enabled
 (``NUMBA_ENABLE_CUDASIM=1``; no GPU, no GL: the kernels write into a plain uint8
@@ -27,7 +27,8 @@ def _f32(a):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("SOLITON_SOLVER_REF"), required="SOLITON_SOLVER_REF" not in os.environ,
+                    help="root of the reference soliton_solver checkout (or set SOLITON_SOLVER_REF)")
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
     args = ap.parse_args()
     os.environ["NUMBA_ENABLE_CUDASIM"] = "1"

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference checkout (it is NOT needed at test time):
 
-    python tests/golden/make_golden_dat.py --ref /root/reference --out tests/golden
+    python tests/golden/make_golden_dat.py --ref <reference checkout> --out tests/golden
 
 The writers are plain Python (no GPU, no Numba kernel), so they are imported and
 called directly: ``output_field_dat``, ``output_density_data_dat``,
@@ -33,7 +33,8 @@ def edge_values():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("SOLITON_SOLVER_REF"), required="SOLITON_SOLVER_REF" not in os.environ,
+                    help="root of the reference soliton_solver checkout (or set SOLITON_SOLVER_REF)")
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
     args = ap.parse_args()
     sys.path.insert(0, args.ref)

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference checkout (it is NOT needed at test time):
 
-    python tests/golden/make_golden_init.py --ref /root/reference --out tests/golden
+    python tests/golden/make_golden_init.py --ref <reference checkout> --out tests/golden
 
 With Numba's CUDA simulator (``NUMBA_ENABLE_CUDASIM=1``; no GPU, no GL) it builds
 each theory's coordinate grid with the theory's ``create_grid_kernel`` and runs, per
@@ -37,7 +37,8 @@ THEORIES = {
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("SOLITON_SOLVER_REF"), required="SOLITON_SOLVER_REF" not in os.environ,
+                    help="root of the reference soliton_solver checkout (or set SOLITON_SOLVER_REF)")
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
     args = ap.parse_args()
     os.environ["NUMBA_ENABLE_CUDASIM"] = "1"

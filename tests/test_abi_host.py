@@ -28,12 +28,24 @@ def test_library_exports_every_declared_symbol():
     assert lib.ss_abi_version() == 1
 
 
-def test_integration_guide_lists_every_entry_point():
-    """Every entry point the header declares has a row (or a mention) in the integration
-    guide, which says which reference interface it replaces."""
-    guide = open(os.path.join(os.path.dirname(HEADER), os.pardir, "INTEGRATION.md")).read()
-    missing = [n for n in _declared() if n not in guide]
-    assert not missing, missing
+def _prototypes():
+    """{name: number of parameters} of every entry point the header declares."""
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for name, params in re.findall(r"^\s*(?:int|const char \*)\s*(ss_\w+)\s*\(([^)]*)\)\s*;", src, flags=re.M):
+        params = params.strip()
+        out[name] = 0 if params in ("", "void") else len(params.split(","))
+    return out
+
+
+def test_binding_signatures_match_the_header():
+    """The ctypes signature table declares every header entry point with the header's
+    number of parameters (a mismatch would pass garbage through the C ABI)."""
+    protos = _prototypes()
+    assert set(protos) == set(_declared())
+    for name, n in protos.items():
+        args, _ = nat._SIG[name]
+        assert len(args) == n, (name, len(args), n)
 
 
 def _create(theory_name, **kw):

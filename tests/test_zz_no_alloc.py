@@ -1,12 +1,15 @@
 """The allocation-free energy entry point, ss_energy_noalloc.
 
-It serves callers that cannot allocate device memory when they need an energy
-(during CUDA-graph stream capture, inside a host that owns all device memory, or
-in a loop that must not let cudaMalloc synchronise the device): its scratch is a
+It serves callers that cannot allocate device memory when they need an energy: a
+host whose memory manager owns all device memory, or an interactive loop that must
+not call cudaMalloc/cudaFree because they synchronise the device.  Its scratch is a
 static device array.  Here it is called through the C ABI twice in a row, on two
 different fields, and each result is compared with the existing ss_energy entry
 point (which uses a caller-allocated workspace) at the tolerance the other energy
-tests use (1e-10 relative).  This file is collected last on purpose.
+tests use (1e-10 relative); the device's free memory and torch's allocations are
+unchanged across the calls; a lattice of exactly the maximum tile count, whose last
+partial sits at the end of the array, matches too.  This file is collected last on
+purpose.
 """
 import ctypes
 
@@ -53,11 +56,32 @@ def test_noalloc_energy_matches_workspace_energy_twice(name, kw, precision):
     p_i, p_f = theory.params.pack_device_params(rp)
     dtype = torch.float32 if precision == "fp32" else torch.float64
     s = Solver(theory.kernels.THEORY_ID, p_i, p_f, precision)
-    for seed in (1, 2):  # two calls in a row: the static scratch keeps the previous call's contents
-        f = _field(rp, seed, dtype)
-        want = s.energy(f)
-        got = _noalloc_energy(theory.kernels.THEORY_ID, p_i, p_f, precision, f)
-        assert abs(got - want) <= 1e-10 * max(1.0, abs(want)), (seed, got, want)
+    fields = [_field(rp, seed, dtype) for seed in (1, 2)]
+    want = [s.energy(f) for f in fields]
+    _noalloc_energy(theory.kernels.THEORY_ID, p_i, p_f, precision, fields[0])  # loads the module
+    torch.cuda.synchronize()
+    free0, alloc0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
+    # two calls in a row: the static scratch keeps the previous call's contents
+    got = [_noalloc_energy(theory.kernels.THEORY_ID, p_i, p_f, precision, f) for f in fields]
+    assert torch.cuda.mem_get_info()[0] == free0 and torch.cuda.memory_allocated() == alloc0
+    for g, w in zip(got, want):
+        assert abs(g - w) <= 1e-10 * max(1.0, abs(w)), (g, w)
+
+
+def test_noalloc_energy_at_the_maximum_tile_count():
+    """512 x 131008 sites = 32 x 2047 = 65504 tiles of 16 x 64, the largest lattice the
+    static scratch takes: its last partial fills the array's last slot."""
+    theory = load_theory("Baby Skyrme")
+    rp = theory.params.default_params(xlen=512, ylen=131008, lsx=0.1, lsy=0.1, unit_magnetization=True).resolved()
+    p_i, p_f = theory.params.pack_device_params(rp)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    f = 0.2 * torch.randn(3, rp.xlen * rp.ylen, device="cuda", generator=g)
+    f[2] += 1.0
+    f = (f / f.norm(dim=0)).reshape(-1).contiguous()
+    want = Solver(theory.kernels.THEORY_ID, p_i, p_f, "fp32").energy(f)
+    for _ in range(2):
+        got = _noalloc_energy(theory.kernels.THEORY_ID, p_i, p_f, "fp32", f)
+        assert abs(got - want) <= 1e-10 * max(1.0, abs(want)), (got, want)
 
 
 def test_noalloc_rejects_lattices_beyond_the_static_scratch():
