@@ -68,7 +68,7 @@ def _workload_params(load_theory, n, spacing, B, demag):
     th = load_theory("Chiral magnet")
     size = spacing * (n - 1)
     p = th.params.default_params(xlen=n, ylen=n, xsize=size, ysize=size, J=40e-12, K=0.8e6, D=4e-3, M=580e3,
-                                 B=B, dmi_term="Heusler", demag=demag, unit_magnetization=True, killkinen=False)
+                                 B=B, dmi_term="Heusler", demag=demag, unit_magnetization=True, killkinen=True)
     return th, p
 
 
@@ -138,6 +138,7 @@ def numba_gpu_flow_steps(n=512, steps=20, warmup=2):
 if __name__ == "__main__":
     import json
     if len(sys.argv) > 1 and sys.argv[1] == "gpu":
-        print(json.dumps(numba_gpu_flow_steps(int(sys.argv[2]) if len(sys.argv) > 2 else 512)))
+        print(json.dumps(numba_gpu_flow_steps(int(sys.argv[2]) if len(sys.argv) > 2 else 512,
+                                              int(sys.argv[3]) if len(sys.argv) > 3 else 20)))
     else:
         print(json.dumps(time_flow_steps(n_proc=int(sys.argv[1]) if len(sys.argv) > 1 else 2)))

@@ -77,6 +77,14 @@ extern "C" {
 #define SS_RENDER_GRAY 1          /* core/colormaps.py render_gray_density_to_rgba */
 #define SS_RENDER_MAGNETIZATION 2 /* core/colormaps.py render_magnetization_to_rgba */
 
+/* diagnostic densities for ss_field_density (gauge theories) */
+#define SS_DENSITY_HIGGS 0            /* |psi|^2: Ginzburg-Landau compute_norm_higgs_kernel */
+#define SS_DENSITY_HIGGS1 1           /* |psi1|^2: s+id compute_norm_higgs1_kernel */
+#define SS_DENSITY_HIGGS2 2           /* |psi2|^2: s+id compute_norm_higgs2_kernel */
+#define SS_DENSITY_PHASE_DIFFERENCE 3 /* cos(arg psi1 - arg psi2): s+id compute_phase_difference_kernel */
+#define SS_DENSITY_SUPERCURRENT 4     /* 2 planes: dxy A2 - dyy A1, dxy A1 - dxx A2 (both gauge theories) */
+#define SS_DENSITY_MAGNETIC_FIELD 5   /* (dx A2 - dy A1) dA/(2 pi Q): s+id compute_magnetic_field_kernel */
+
 /* initial conditions (ss_initialize, ss_insert_soliton) */
 #define SS_INIT_GROUND 0   /* create_ground_state_kernel */
 #define SS_INIT_ANSATZ 1   /* create_initial_configuration_kernel */
@@ -235,6 +243,24 @@ int ss_render_rgba(int kind, const void *src, int precision, int xlen, int ylen,
  * theories/ginzburg_landau_superconductor/kernels.py:181-215). */
 int ss_charge_density(ss_handle *h, const void *field, int which, double *density);
 int ss_charge(ss_handle *h, const void *field, int which, double *out);
+/* Copy of a field of the handle's lattice and theory from src (SS_FP32 or SS_FP64 /
+ * SS_PLAIN_FP64 elements, `src_precision`) into dst (`dst_precision`), on the handle's
+ * stream (asynchronous; needs no workspace).  With project != 0, each site's
+ * unit-vector components are divided by their FP64 norm first (theories with the
+ * constraint and unit_magnetization set; the normalisation of the reference's RK4
+ * finalize, core/integrator.py:151-189); the result is rounded once to dst's type.
+ * Used to hand a relaxation from FP32 to FP64 fields and back.  In place only for
+ * equal element types.  No reference counterpart (the reference is FP64 only). */
+int ss_convert_field(ss_handle *h, const void *src, int src_precision, void *dst, int dst_precision, int project);
+/* Diagnostic density of `field` (element type of the handle) into the device array
+ * `out` (double; N sites, 2 N for SS_DENSITY_SUPERCURRENT: the x plane, then the y
+ * plane), asynchronous on the handle's stream; needs no workspace.  Replaces the
+ * Simulation helpers compute_higgs_density, compute_higgs1_density,
+ * compute_higgs2_density, compute_phase_difference_density, supercurrent and
+ * magnetic_field (soliton_solver/core/simulation.py:211-300,301-318,370-386) and the
+ * kernels they launch (theories/ginzburg_landau_superconductor/kernels.py:218-340,
+ * theories/anisotropic_superconductor/kernels.py:280-553). */
+int ss_field_density(ss_handle *h, const void *field, int kind, double *out);
 /* Partial derivative dE/dc of the discrete energy with respect to a coupling at
  * fixed field.  At a relaxed (stationary) field this is dE_min/dc by the envelope
  * theorem.  No reference counterpart: a new capability of this backend. */

@@ -688,6 +688,33 @@ def charge(theory, F, p_i, p_f, which):
     return reference_sum(charge_density(theory, F, p_i, p_f, which))
 
 
+def field_density(theory, F, p_i, p_f, kind):
+    """Diagnostic densities of the gauge theories (Simulation's output helpers).
+
+    'higgs'      |psi|^2, ginzburg_landau_superconductor/kernels.py:218-272
+    'higgs1'     |psi1|^2, anisotropic_superconductor/kernels.py:315-369
+    'higgs2'     |psi2|^2, anisotropic_superconductor/kernels.py:372-426
+    'phase'      cos(atan2(psi1) - atan2(psi2)), anisotropic_superconductor/kernels.py:497-553
+    'supercurrent' (2, X, Y): (d2[1,0,A2] - d2[1,1,A1], d2[0,1,A1] - d2[0,0,A2]),
+                 ginzburg_landau_superconductor/kernels.py:275-340 (second derivatives of
+                 the gauge fields only, with the mixed-derivative ring)
+    'magnetic'   the vortex density with which = 2 (compute_magnetic_field_kernel,
+                 anisotropic_superconductor/kernels.py:280-312)
+    """
+    if kind in ("higgs", "higgs1", "higgs2"):
+        a = 4 if kind == "higgs2" else 2
+        return F[a] * F[a] + F[a + 1] * F[a + 1]
+    if kind == "phase":
+        return np.cos(np.arctan2(F[3], F[2]) - np.arctan2(F[5], F[4]))
+    ng = int(p_i[11] if theory == "ginzburg_landau_superconductor" else p_i[12])
+    if kind == "supercurrent":
+        d2 = second_derivatives(F, p_i, p_f, comps=range(ng))
+        return np.stack([d2[1, 0, 1] - d2[1, 1, 0], d2[0, 1, 0] - d2[0, 0, 1]])
+    if kind == "magnetic":
+        return charge_density(theory, F, p_i, p_f, "vortex")
+    raise ValueError(kind)
+
+
 def rk4_stage(V, l_in, F, k_prev, factor, p_f):
     """do_rk4_step_kernel, core/integrator.py:51-96: returns (k_out, Temp)."""
     dt = float(p_f[5])

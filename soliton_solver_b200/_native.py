@@ -50,6 +50,14 @@ SS_RENDER_JET = 0
 SS_RENDER_GRAY = 1
 SS_RENDER_MAGNETIZATION = 2
 
+# diagnostic densities (ss_field_density)
+SS_DENSITY_HIGGS = 0
+SS_DENSITY_HIGGS1 = 1
+SS_DENSITY_HIGGS2 = 2
+SS_DENSITY_PHASE_DIFFERENCE = 3
+SS_DENSITY_SUPERCURRENT = 4
+SS_DENSITY_MAGNETIC_FIELD = 5
+
 # couplings
 SS_COUPLING_KAPPA = 0
 SS_COUPLING_MPI = 1
@@ -110,6 +118,8 @@ _SIG = {
     "ss_charge_density": ([_P, _P, _I, _P], _I),
     "ss_charge": ([_P, _P, _I, ctypes.POINTER(_D)], _I),
     "ss_coupling_grad": ([_P, _P, _I, ctypes.POINTER(_D)], _I),
+    "ss_field_density": ([_P, _P, _I, _P], _I),
+    "ss_convert_field": ([_P, _P, _I, _P, _I, _I], _I),
     "ss_energy_noalloc": ([_I, _P, _I, _P, _I, _I, _P, ctypes.POINTER(_D), _P], _I),
     "ss_rk4_stage": ([_P, _P, _P, _P, _P, _P, _P, _D], _I),
     "ss_batch_create": ([_I, _I, _P, _I, _P, _I, _I, ctypes.POINTER(_P)], _I),

@@ -44,8 +44,19 @@ def _solver(theory_id, field, p_i, p_f):
     return solver_for(theory_id, p_i, p_f, f.dtype, f.device), f
 
 
-def make_kernels(theory_id: int, charges=()):
-    """Hook adapters of one theory: returns a dict name -> Launch."""
+def _geometry_solver(theory_id, field, p_i):
+    """Solver for hooks that pass only p_i (pointwise densities): the float parameters
+    are never read by those kernels, so unit placeholders stand in for them."""
+    import numpy as np
+    from soliton_solver_b200.core.solver import _to_host
+    pf = np.ones(32)
+    return _solver(theory_id, field, _to_host(p_i), pf)
+
+
+def make_kernels(theory_id: int, charges=(), densities=()):
+    """Hook adapters of one theory: returns a dict name -> Launch.  ``densities`` names
+    the diagnostic densities the theory's kernels module provides ('higgs', 'higgs1',
+    'higgs2', 'phase', 'supercurrent', 'magnetic')."""
 
     def do_gradient_step_kernel(l_out, Field, d1fd1x, d2fd2x, EnergyGradient, p_i, p_f):
         s, f = _solver(theory_id, Field, p_i, p_f)
@@ -99,6 +110,24 @@ def make_kernels(theory_id: int, charges=()):
             s, f = _solver(theory_id, Field, p_i, p_f)
             s.charge_density(f, "vortex", as_tensor(en))
         out["compute_vortex_number_kernel"] = Launch(compute_vortex_number_kernel, "compute_vortex_number_kernel")
+    pointwise = {"higgs": "compute_norm_higgs_kernel", "higgs1": "compute_norm_higgs1_kernel",
+                 "higgs2": "compute_norm_higgs2_kernel", "phase": "compute_phase_difference_kernel"}
+    for kind, name in pointwise.items():
+        if kind in densities:
+            def pointwise_kernel(en, Field, p_i, _kind=kind):
+                s, f = _geometry_solver(theory_id, Field, p_i)
+                s.field_density(f, _kind, as_tensor(en))
+            out[name] = Launch(pointwise_kernel, name)
+    if "supercurrent" in densities:
+        def compute_supercurrent_kernel(Field, d2fd2x, Supercurrent, p_i, p_f):
+            s, f = _solver(theory_id, Field, p_i, p_f)
+            s.field_density(f, "supercurrent", as_tensor(Supercurrent))
+        out["compute_supercurrent_kernel"] = Launch(compute_supercurrent_kernel, "compute_supercurrent_kernel")
+    if "magnetic" in densities:
+        def compute_magnetic_field_kernel(Field, d1fd1x, MagneticFluxDensity, p_i, p_f):
+            s, f = _solver(theory_id, Field, p_i, p_f)
+            s.field_density(f, "magnetic", as_tensor(MagneticFluxDensity))
+        out["compute_magnetic_field_kernel"] = Launch(compute_magnetic_field_kernel, "compute_magnetic_field_kernel")
     return out
 
 

@@ -47,6 +47,35 @@ class Simulation:
         self._make_solver()
         self.last_energy = math.nan
 
+    # The reference's Simulation allocates the derivative, RK4 and reduction scratch that
+    # its hooks pass around (soliton_solver/core/simulation.py:91-115).  The fused kernels
+    # never read them, so they are allocated only when a caller touches them, with the
+    # reference's sizes: reference-style code such as
+    # observables.compute_energy(sim.Field, sim.d1fd1x, sim.en, ...) runs unchanged.
+    def __getattr__(self, name):
+        sizes = self._scratch_sizes()
+        if name not in sizes:
+            raise AttributeError(f"{type(self).__name__!s} has no attribute {name!r}")
+        n, dtype = sizes[name]
+        t = torch.zeros(int(n), dtype=dtype, device=self.__dict__["device"])
+        self.__dict__[name] = t
+        return t
+
+    def _scratch_sizes(self):
+        rp = self.__dict__.get("rp")
+        if rp is None:
+            return {}
+        field_dtype = torch.float32 if self.__dict__.get("precision") == "fp32" else torch.float64
+        nc, nf, N = rp.number_coordinates, rp.number_total_fields, rp.dim_grid
+        ng = int(getattr(rp, "number_gauge_fields", 0))
+        out = {f"{k}{i}": (rp.dim_fields, field_dtype) for k in ("k", "l") for i in range(1, 5)}
+        out.update(Temp=(rp.dim_fields, field_dtype), d1fd1x=(nc * nf * N, torch.float64),
+                   d2fd2x=(nc * nc * nf * N, torch.float64), gridsum_partial=((N + 1023) // 1024, torch.float64),
+                   max_partial=((rp.dim_fields + 1023) // 1024, torch.float64),
+                   MagneticFluxDensity=(ng * N if ng > 0 else 1, torch.float64),
+                   Supercurrent=(ng * N if ng > 0 else 1, torch.float64))
+        return out
+
     # ------------------------------------------------------------------ setup
     def _make_solver(self):
         self.solver = Solver(self.kernels.THEORY_ID, self.p_i_h, self.p_f_h, self.precision, self.device)
@@ -102,7 +131,138 @@ class Simulation:
             self.last_energy = float(E[-1])
         return E, err
 
-    # ------------------------------------------------------------------ observables
+    def minimize(self, tol: float = 1e-6, max_steps: int = 1_000_000, schedule: str | None = None,
+                 chunk: int | None = None, plateau: float = 1e-9, record: bool = False) -> dict:
+        """Relax sim.Field by arrested Newton flow until the stage-4 gradient max
+        |dE/dphi| (the reference's err) drops below ``tol``.
+
+        The reference documents ``sim.minimize(tol=...)`` (soliton_solver/core/
+        simulation.py:8,39) but relaxes by calling ``E, err = sim.step(E)`` until err <
+        tol (core/integrator.py:217-348); this runs that loop on the device in chunks of
+        ``chunk`` steps (one host synchronisation per chunk, CUDA-graph replays).
+
+        schedule
+          "fp64"       FP64 fields throughout (an FP64 copy of an FP32 Simulation's field).
+          "fp32"       FP32 fields with FP64 energy sums; stops at tol or at the FP32
+                       energy plateau (see below), whichever comes first.
+          "fp32+fp64"  (default for FP32 Simulations) the FP32 flow until tol or its
+                       plateau, then the same flow on an FP64 copy of the state, each
+                       site's unit vector renormalised in FP64, until tol.  FP32 steps
+                       run at about a third of the FP64 cost; FP32 rounding bounds how far
+                       they get (the gradient stalls at ~eps/h^2), and the FP64 steps
+                       finish from there.
+        A phase reaches its plateau when its energy falls by less than ``plateau`` x |E|
+        over two chunks in a row.  ``max_steps`` bounds the total.  Needs the arrested
+        flow (killkinen on).
+
+        Returns a dict: energy (FP64 observable of the final field), err, converged,
+        steps, and per phase its precision, steps, wall seconds, start/end energy, end
+        err and stop reason.  The final field is written to sim.Field (rounded to its
+        element type) and kept in FP64 as sim.Field64 after an FP64 phase.  With
+        ``record`` the result also holds the per-step energy / err trajectories and, for
+        FP32 phases, the FP64 projected energy at every chunk end."""
+        import time
+
+        if not int(self.p_i_h[7]):
+            raise ValueError("minimize needs the arrested flow: set killkinen=True in the parameters")
+        if schedule is None:
+            schedule = "fp32+fp64" if self.precision == "fp32" else "fp64"
+        if schedule not in ("fp64", "fp32", "fp32+fp64"):
+            raise ValueError("schedule must be 'fp64', 'fp32' or 'fp32+fp64'")
+        if schedule != "fp64" and self.precision != "fp32":
+            raise ValueError(f"schedule {schedule!r} needs an FP32 Simulation")
+        N = self.rp.dim_grid
+        chunk = int(chunk) if chunk else (1000 if N <= (1 << 20) else 200)
+        out = {"schedule": schedule, "tol": tol, "phases": [], "steps": 0}
+        traj = {"energy": [], "err": [], "precision": [], "projected": []}
+        budget = int(max_steps)
+        E_start = self.observables()["energy"] if math.isnan(self.last_energy) else self.last_energy
+
+        def phase(solver, field, vel, prec, E0, budget, project_chunks):
+            t0 = time.perf_counter()
+            Et = torch.empty(chunk, dtype=torch.float64, device=self.device)
+            rt = torch.empty(chunk, dtype=torch.float64, device=self.device)
+            steps, hits, stop = 0, 0, "max_steps"
+            E_prev, E, err = E0, E0, math.inf
+            graph = False
+            while steps < budget:
+                n = min(chunk, budget - steps)
+                if n == chunk and steps > 0:
+                    if not graph:
+                        solver.capture(chunk, Et, rt)
+                        graph = True
+                    solver.replay()
+                else:
+                    solver.step_async(n, E0 if steps == 0 else math.nan, Et, rt)
+                Eh = Et[:n].cpu().numpy()
+                rh = rt[:n].cpu().numpy()
+                solver.check_status()
+                if record:
+                    traj["energy"].append(Eh.copy())
+                    traj["err"].append(rh.copy())
+                    traj["precision"].append(np.full(n, 32 if prec == "fp32" else 64, np.int8))
+                    if project_chunks:
+                        traj["projected"].append((out["steps"] + steps + n, solver.energy_projected(field)))
+                below = np.nonzero(np.abs(rh) < tol)[0]
+                if below.size:
+                    steps += int(below[0]) + 1
+                    E, err, stop = float(Eh[below[0]]), float(rh[below[0]]), "tol"
+                    break
+                steps += n
+                E, err = float(Eh[-1]), float(rh[-1])
+                hits = hits + 1 if E_prev - E < plateau * abs(E) else 0
+                E_prev = E
+                if hits >= 2 and prec == "fp32":
+                    stop = "plateau"
+                    break
+            torch.cuda.synchronize(self.device)
+            rec = {"precision": prec, "steps": steps, "wall_s": time.perf_counter() - t0, "energy_start": E0,
+                   "energy_end": E, "err_end": err, "stop": stop}
+            out["phases"].append(rec)
+            out["steps"] += steps
+            return rec
+
+        if schedule in ("fp32", "fp32+fp64"):
+            rec = phase(self.solver, self.Field, self.Velocity, "fp32", E_start, budget, record)
+            budget -= rec["steps"]
+            E_start = rec["energy_end"]
+            if schedule == "fp32" or rec["stop"] == "tol" or budget <= 0:
+                out.update(energy=self.solver.energy(self.Field), err=rec["err_end"], converged=rec["stop"] == "tol")
+                self.last_energy = rec["energy_end"]
+                return self._finish_minimize(out, traj, record)
+        # FP64 phase: on the Simulation's own buffers, or on a projected FP64 copy
+        if self.precision == "fp32":
+            F64 = torch.empty(self.Field.numel(), dtype=torch.float64, device=self.device)
+            V64 = torch.empty_like(F64)
+            self.solver.convert(self.Field, F64, project=True)
+            self.solver.convert(self.Velocity, V64, project=False)
+            s64 = Solver(self.kernels.THEORY_ID, self.p_i_h, self.p_f_h, "fp64", self.device)
+            s64.bind(F64, V64)
+            E_start = s64.energy(F64)
+        else:
+            F64, V64, s64 = self.Field, self.Velocity, self.solver
+        rec = phase(s64, F64, V64, "fp64", E_start, budget, False)
+        out.update(energy=s64.energy(F64), err=rec["err_end"], converged=rec["stop"] == "tol")
+        if F64 is not self.Field:
+            s64.convert(F64, self.Field, project=False)
+            s64.convert(V64, self.Velocity, project=False)
+            self.Field64 = F64
+            self.solver.rebind()  # the FP32 flow restarts its arrest history from the new state
+        self.last_energy = out["energy"]
+        torch.cuda.synchronize(self.device)
+        return self._finish_minimize(out, traj, record)
+
+    @staticmethod
+    def _finish_minimize(out, traj, record):
+        if record:
+            out["trajectory"] = {"energy": np.concatenate(traj["energy"]) if traj["energy"] else np.empty(0),
+                                 "err": np.concatenate(traj["err"]) if traj["err"] else np.empty(0),
+                                 "precision": np.concatenate(traj["precision"]) if traj["precision"] else
+                                 np.empty(0, np.int8),
+                                 "projected": np.array(traj["projected"], dtype=np.float64).reshape(-1, 2)}
+        return out
+
+    # ------------------------------------------------------------------ observables    # ------------------------------------------------------------------ observables
     def observables(self):
         """Energy plus every charge the theory's observables module provides
         (soliton_solver/core/simulation.py:168-192)."""
@@ -127,12 +287,11 @@ class Simulation:
         return self.solver.energy_projected(self.Field)
 
     def save_output(self, output_dir: str | None = None, precision: int = 32):
-        """The theory's .dat output bundle (soliton_solver/core/simulation.py save_output):
+        """The theory's .dat output bundle (soliton_solver/core/simulation.py:411-516):
         lattice sizes and vectors, the field dump and the component grids of the field,
-        the energy density and the theory's charge densities, formatted on the GPU.
-        Arrays this backend does not compute (supercurrent, magnetic flux density) are
-        passed as None and their files skipped, as the reference skips missing arrays.
-        The default directory is the theory package's ``results``."""
+        the energy density, the charge densities and, for the gauge theories, the Higgs
+        densities, supercurrent and magnetic flux density, formatted on the GPU.  The
+        default directory is the theory package's ``results``."""
         import inspect
         import os
         if output_dir is None:
@@ -141,14 +300,26 @@ class Simulation:
         self.kernels.create_grid_kernel[None, None](self.grid, self.p_i_h, self.p_f_h)
         om = self.observables_mod
         dens = {"h_EnergyDensity": self.solver.energy_density(self.Field).clone()}
+        for name, method in (("h_MagneticFluxDensity", self.magnetic_field), ("h_Supercurrent", self.supercurrent)):
+            try:
+                dens[name] = method().clone()
+            except AttributeError:  # the theory has no such kernel: the reference skips it too
+                pass
         if hasattr(om, "compute_skyrmion_number"):
             dens["h_BaryonDensity"] = self.solver.charge_density(self.Field, "skyrmion").clone()
         if hasattr(om, "compute_magnetic_charge"):
             dens["h_MagneticChargeDensity"] = self.solver.charge_density(self.Field, "magnetic").clone()
         if hasattr(om, "compute_vortex_number"):
             dens["h_VortexDensity"] = self.solver.charge_density(self.Field, "vortex").clone()
-        kwargs = dict(output_dir=output_dir, h_Field=self.Field, h_grid=self.grid, h_Supercurrent=None,
-                      h_MagneticFluxDensity=None, xlen=int(self.p_i_h[0]), ylen=int(self.p_i_h[1]),
+        if hasattr(self.kernels, "compute_norm_higgs_kernel"):
+            dens["h_HiggsDensity"] = self.solver.field_density(self.Field, "higgs").clone()
+        if hasattr(self.kernels, "compute_norm_higgs1_kernel"):
+            dens["h_Higgs1Density"] = self.solver.field_density(self.Field, "higgs1").clone()
+            dens["h_Higgs2Density"] = self.solver.field_density(self.Field, "higgs2").clone()
+        dens.setdefault("h_Supercurrent", None)
+        dens.setdefault("h_MagneticFluxDensity", None)
+        kwargs = dict(output_dir=output_dir, h_Field=self.Field, h_grid=self.grid, xlen=int(self.p_i_h[0]),
+                      ylen=int(self.p_i_h[1]),
                       number_coordinates=int(self.p_i_h[3]), number_total_fields=int(self.p_i_h[4]),
                       precision=precision, **dens)
         accepted = set(inspect.signature(self.theory.io.output_data_bundle).parameters)
@@ -157,6 +328,41 @@ class Simulation:
     def compute_energy_density(self):
         self.solver.energy_density(self.Field, self.en)
         torch.cuda.synchronize(self.device)
+
+    # diagnostic densities of the gauge theories (soliton_solver/core/simulation.py:211-386)
+    def _kernel_density(self, kernel_name, kind, out):
+        if not hasattr(self.kernels, kernel_name):
+            raise AttributeError(f"theory kernels have no {kernel_name}")
+        self.solver.field_density(self.Field, kind, out)
+        torch.cuda.synchronize(self.device)
+        return out
+
+    def compute_higgs_density(self):
+        """|psi|^2 per site into ``en`` (compute_norm_higgs_kernel)."""
+        self._kernel_density("compute_norm_higgs_kernel", "higgs", self.en)
+
+    def compute_higgs1_density(self):
+        """|psi1|^2 per site into ``en`` (compute_norm_higgs1_kernel)."""
+        self._kernel_density("compute_norm_higgs1_kernel", "higgs1", self.en)
+
+    def compute_higgs2_density(self):
+        """|psi2|^2 per site into ``en`` (compute_norm_higgs2_kernel)."""
+        self._kernel_density("compute_norm_higgs2_kernel", "higgs2", self.en)
+
+    def compute_phase_difference_density(self):
+        """cos(arg psi1 - arg psi2) per site into ``en`` (compute_phase_difference_kernel)."""
+        self._kernel_density("compute_phase_difference_kernel", "phase", self.en)
+
+    def magnetic_field(self):
+        """Magnetic flux density (dx A2 - dy A1) dA/(2 pi Q) into the first N entries of
+        ``MagneticFluxDensity`` and returned (compute_magnetic_field_kernel; the
+        Ginzburg-Landau theory has none, as in the reference)."""
+        return self._kernel_density("compute_magnetic_field_kernel", "magnetic", self.MagneticFluxDensity)
+
+    def supercurrent(self):
+        """Supercurrent (dxy A2 - dyy A1, dxy A1 - dxx A2) into ``Supercurrent`` (x plane,
+        then y plane) and returned (compute_supercurrent_kernel)."""
+        return self._kernel_density("compute_supercurrent_kernel", "supercurrent", self.Supercurrent)
 
     def compute_magnetic_flux_density(self, which=2):
         self.solver.charge_density(self.Field, "vortex", self.en)

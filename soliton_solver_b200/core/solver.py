@@ -17,6 +17,9 @@ import torch
 from soliton_solver_b200 import _native as nat
 
 _CHARGES = {"skyrmion": nat.SS_CHARGE_SKYRMION, "magnetic": nat.SS_CHARGE_MAGNETIC, "vortex": nat.SS_CHARGE_VORTEX}
+_DENSITIES = {"higgs": nat.SS_DENSITY_HIGGS, "higgs1": nat.SS_DENSITY_HIGGS1, "higgs2": nat.SS_DENSITY_HIGGS2,
+              "phase": nat.SS_DENSITY_PHASE_DIFFERENCE, "supercurrent": nat.SS_DENSITY_SUPERCURRENT,
+              "magnetic": nat.SS_DENSITY_MAGNETIC_FIELD}
 _COUPLINGS = {"kappa": nat.SS_COUPLING_KAPPA, "mpi": nat.SS_COUPLING_MPI, "Lambda": nat.SS_COUPLING_LAMBDA,
               "coup_K": nat.SS_COUPLING_COUP_K, "coup_h": nat.SS_COUPLING_COUP_H,
               "coup_mu": nat.SS_COUPLING_COUP_MU}
@@ -238,6 +241,35 @@ class Solver:
         self._check(out, torch.float64)
         with torch.cuda.device(self.device):
             nat.check(self._lib.ss_charge_density(self._h, _ptr(field), _CHARGES[which], _ptr(out)))
+        return out
+
+    def convert(self, src, dst, project: bool = True):
+        """Copy `src` into `dst` (FP32 or FP64 tensors of this lattice, either way round),
+        with each site's unit vector renormalised in FP64 first when `project` (see
+        ss_convert_field).  Asynchronous on the solver's stream."""
+        for t in (src, dst):
+            if not isinstance(t, torch.Tensor) or t.dtype not in (torch.float32, torch.float64) or \
+                    t.device != self.device or not t.is_contiguous() or t.numel() != self.nf * self.N:
+                raise ValueError(f"convert needs contiguous FP32/FP64 tensors of {self.nf * self.N} entries on "
+                                 f"{self.device}")
+        code = {torch.float32: nat.SS_FP32, torch.float64: nat.SS_FP64}
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_convert_field(self._h, _ptr(src), code[src.dtype], _ptr(dst), code[dst.dtype],
+                                                 1 if project else 0))
+        return dst
+
+    def field_density(self, field, kind: str, out=None):
+        """Diagnostic density of a gauge theory (see ss_field_density): 'higgs', 'higgs1',
+        'higgs2', 'phase', 'magnetic' (N doubles) or 'supercurrent' (2 N: x plane, y plane).
+        Asynchronous on the solver's stream."""
+        self._check(field)
+        n = 2 * self.N if kind == "supercurrent" else self.N
+        out = out if out is not None else torch.empty(n, dtype=torch.float64, device=self.device)
+        self._check(out, torch.float64)
+        if out.numel() < n:
+            raise ValueError(f"output buffer needs {n} entries")
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_field_density(self._h, _ptr(field), _DENSITIES[kind], _ptr(out)))
         return out
 
     def coupling_grad(self, field, which: str) -> float:

@@ -18,6 +18,7 @@
 #include "batch.cuh"
 #include "render.cuh"
 #include "init.cuh"
+#include "observe.cuh"
 #include "text.cuh"
 #include "theories.cuh"
 
@@ -667,7 +668,7 @@ struct Fused {
   // for every precision (two FP32 l buffers, or one FP64 one) and is free between steps.
   static int energy_projected(ss_handle* h, const void* field) {
     double* copy = (double*)h->l[0];
-    project_kernel<R, TH::NF, TH::NMAG><<<grid_1d(h->G.N), 256, 0, h->stream>>>(
+    convert_kernel<R, double, TH::NF, TH::NMAG><<<grid_1d(h->G.N), 256, 0, h->stream>>>(
         (const R*)field, copy, h->G.N, TH::CONSTRAINED && h->G.unit_mag);
     CK(cudaGetLastError());
     return Fused<TH, double>::energy(h, copy);
@@ -1294,6 +1295,41 @@ int ss_coupling_grad(ss_handle* h, const void* field, int coupling, double* out)
   rc = fused_density(h, field, nullptr, true, D_COUPLING, coupling);
   if (rc) return rc;
   return scalar_result(h, out);
+}
+
+int ss_convert_field(ss_handle* h, const void* src, int src_precision, void* dst, int dst_precision, int project) {
+  if (!h || !src || !dst) return fail(SS_ERR_ARG, "NULL argument");
+  auto is_prec = [](int p) { return p == SS_FP32 || p == SS_FP64 || p == SS_PLAIN_FP64; };
+  if (!is_prec(src_precision) || !is_prec(dst_precision)) return fail(SS_ERR_ARG, "unknown precision");
+  const bool s32 = src_precision == SS_FP32, d32 = dst_precision == SS_FP32;
+  if (src == dst && s32 != d32) return fail(SS_ERR_ARG, "in-place conversion needs equal element types");
+  return dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    const int norm = project && TH::CONSTRAINED && h->G.unit_mag;
+    const dim3 g = grid_1d(h->G.N);
+    if (s32 && d32) convert_kernel<float, float, TH::NF, TH::NMAG><<<g, 256, 0, h->stream>>>((const float*)src, (float*)dst, h->G.N, norm);
+    else if (s32) convert_kernel<float, double, TH::NF, TH::NMAG><<<g, 256, 0, h->stream>>>((const float*)src, (double*)dst, h->G.N, norm);
+    else if (d32) convert_kernel<double, float, TH::NF, TH::NMAG><<<g, 256, 0, h->stream>>>((const double*)src, (float*)dst, h->G.N, norm);
+    else convert_kernel<double, double, TH::NF, TH::NMAG><<<g, 256, 0, h->stream>>>((const double*)src, (double*)dst, h->G.N, norm);
+    CK(cudaGetLastError());
+    return SS_OK;
+  });
+}
+
+int ss_field_density(ss_handle* h, const void* field, int kind, double* out) {
+  if (!h || !field || !out) return fail(SS_ERR_ARG, "NULL argument");
+  const bool ah = h->theory == SS_THEORY_GINZBURG_LANDAU, sid = h->theory == SS_THEORY_ANISOTROPIC;
+  const bool ok = (kind == SS_DENSITY_HIGGS && ah) || (kind == SS_DENSITY_SUPERCURRENT && (ah || sid)) ||
+                  ((kind == SS_DENSITY_HIGGS1 || kind == SS_DENSITY_HIGGS2 || kind == SS_DENSITY_PHASE_DIFFERENCE ||
+                    kind == SS_DENSITY_MAGNETIC_FIELD) && sid);
+  if (!ok) return fail(SS_ERR_ARG, "density kind %d not defined for theory %d", kind, h->theory);
+  const double q = ah ? h->P.c[0] : h->P.c[1];
+  if (h->precision == SS_FP32)
+    field_density_kernel<float><<<grid_1d(h->G.N), 256, 0, h->stream>>>((const float*)field, out, kind, h->G, q);
+  else
+    field_density_kernel<double><<<grid_1d(h->G.N), 256, 0, h->stream>>>((const double*)field, out, kind, h->G, q);
+  CK(cudaGetLastError());
+  return SS_OK;
 }
 
 int ss_rk4_stage(ss_handle* h, void* k_out, const void* velocity, const void* l_in, void* temp, const void* field,

@@ -1191,16 +1191,18 @@ __global__ void rk4_finalize_kernel(R* vel, R* phi, const R* k1, const R* k2, co
   }
 }
 
-// FP64 copy of a field with each site's unit-vector components divided by their
-// FP64 norm (the projection the flow applies after every step).  A stored FP32 unit
-// vector cannot hold m3 = 1 - |m_perp|^2/2 once |m_perp| < 2.4e-4: it rounds to 1 and
-// |m|^2 - 1 = |m_perp|^2 > 0 there; the copy restores the constraint to FP64 rounding.
-template <typename R, int NF, int NMAG>
-__global__ void project_kernel(const R* phi, double* out, long long N, int normalize) {
+// Copy of a field in another element type (S -> D), optionally with each site's
+// unit-vector components divided by their FP64 norm (the projection the flow applies
+// after every step).  A stored FP32 unit vector cannot hold m3 = 1 - |m_perp|^2/2 once
+// |m_perp| < 2.4e-4: it rounds to 1 and |m|^2 - 1 = |m_perp|^2 > 0 there; an FP64
+// projected copy restores the constraint to FP64 rounding.  Each site's components are
+// read and normalised in FP64, then rounded once to D.
+template <typename S, typename D, int NF, int NMAG>
+__global__ void convert_kernel(const S* src, D* dst, long long N, int normalize) {
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < N; s += (long long)gridDim.x * blockDim.x) {
     double P[NF];
 #pragma unroll
-    for (int a = 0; a < NF; ++a) P[a] = (double)phi[a * N + s];
+    for (int a = 0; a < NF; ++a) P[a] = (double)src[a * N + s];
     if (NMAG > 0 && normalize) {
       double s2 = 0.0;
 #pragma unroll
@@ -1212,7 +1214,7 @@ __global__ void project_kernel(const R* phi, double* out, long long N, int norma
       }
     }
 #pragma unroll
-    for (int a = 0; a < NF; ++a) out[a * N + s] = P[a];
+    for (int a = 0; a < NF; ++a) dst[a * N + s] = (D)P[a];
   }
 }
 

@@ -117,3 +117,17 @@ def vortices(rp, n=4, sigma=0.0, seed=0, device="cpu"):
     if sigma:
         F = F + _noise(F.shape, sigma, seed + 1, device)
     return F.reshape(-1)
+
+
+def vortex(rp, winding=1, center=None, device="cpu"):
+    """Abelian Higgs: one vortex of winding n at `center` (default: the lattice centre),
+    psi = u1 tanh(r)^|n| e^{i n theta}, A = 0 (a coalesced n-vortex for |n| > 1)."""
+    x, y = _coords(rp, device)
+    cx, cy = center if center is not None else (0.5 * (rp.xlen - 1) * rp.lsx, 0.5 * (rp.ylen - 1) * rp.lsy)
+    dx, dy = x - cx, y - cy
+    r = torch.sqrt(dx * dx + dy * dy)
+    th = torch.atan2(dy, dx)
+    amp = float(getattr(rp, "u1", 1.0)) * torch.tanh(r) ** abs(winding)
+    F = torch.stack([torch.zeros_like(x), torch.zeros_like(x), amp * torch.cos(winding * th),
+                     amp * torch.sin(winding * th)])
+    return F.reshape(-1)

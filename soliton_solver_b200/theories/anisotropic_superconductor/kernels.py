@@ -8,8 +8,9 @@ from soliton_solver_b200.core.hooks import make_kernels
 
 THEORY_ID = _nat.SS_THEORY_ANISOTROPIC
 CHARGES = ('vortex',)
+DENSITIES = ('higgs1', 'higgs2', 'phase', 'supercurrent', 'magnetic')
 CONSTRAINED = False
 
-globals().update(make_kernels(THEORY_ID, CHARGES))
+globals().update(make_kernels(THEORY_ID, CHARGES, DENSITIES))
 
 del do_rk4_kernel  # unconstrained: Simulation uses the core no-constraint finalize

@@ -194,6 +194,34 @@ def main():
         np.savez_compressed(os.path.join(args.out, f"hook_{name}.npz"), **rec)
         print(f"hook_{name}: {time.time() - t0:.1f}s", flush=True)
 
+    # diagnostic densities of the gauge theories through the reference's Simulation helpers
+    for seed, (name, theory, kw) in enumerate(_cases()):
+        if theory not in ("ginzburg_landau_superconductor", "anisotropic_superconductor"):
+            continue
+        if args.only and args.only not in "density_" + name:
+            continue
+        th = load_theory(THEORY_NAMES[theory])
+        sim = Simulation(th.params.default_params(**kw), th)
+        rp = sim.rp
+        F = _random_field(theory, rp, np.random.default_rng(3000 + seed))
+        sim.Field.copy_to_device(F.reshape(-1))
+        rec = dict(theory=theory, p_i=sim.p_i_h, p_f=sim.p_f_h, field=F.reshape(-1))
+        N = rp.xlen * rp.ylen
+        if theory == "ginzburg_landau_superconductor":
+            sim.compute_higgs_density()
+            rec["higgs"] = sim.en.copy_to_host()
+        else:
+            sim.compute_higgs1_density()
+            rec["higgs1"] = sim.en.copy_to_host()
+            sim.compute_higgs2_density()
+            rec["higgs2"] = sim.en.copy_to_host()
+            sim.compute_phase_difference_density()
+            rec["phase"] = sim.en.copy_to_host()
+            rec["magnetic"] = sim.magnetic_field().copy_to_host()[:N]
+        rec["supercurrent"] = sim.supercurrent().copy_to_host()[:2 * N]
+        np.savez_compressed(os.path.join(args.out, f"density_{name}.npz"), **rec)
+        print(f"density_{name}", flush=True)
+
     for seed, (name, theory, kw, prev_e, nsteps) in enumerate(_traj_cases()):
         if args.only and args.only not in name:
             continue

@@ -123,3 +123,21 @@ def test_splusid_condensate_rows_are_not_dE_dpsi():
     for ad, fd in _fd_vs_gradient("ginzburg_landau_superconductor", dict(xlen=64, ylen=68, xsize=6.3, ysize=6.7),
                                   (0, 1, 2, 3)):
         assert abs(ad - fd) <= 1e-3 * abs(fd)
+
+
+DENSITIES = sorted(glob.glob(os.path.join(GOLDEN, "density_*.npz")))
+
+
+@pytest.mark.parametrize("path", DENSITIES, ids=[os.path.basename(p)[8:-4] for p in DENSITIES])
+def test_field_densities(path):
+    """Higgs norms, phase difference, supercurrent and magnetic field of the gauge theories
+    against the reference's Simulation helpers (compute_higgs*_density, supercurrent,
+    magnetic_field, compute_phase_difference_density)."""
+    g = np.load(path)
+    th = str(g["theory"])
+    p_i, p_f = g["p_i"], g["p_f"]
+    F = ref.as_field(g["field"], p_i)
+    kinds = [k for k in ("higgs", "higgs1", "higgs2", "phase", "magnetic", "supercurrent") if k in g]
+    assert "supercurrent" in kinds and len(kinds) >= 2
+    for k in kinds:
+        _close(ref.field_density(th, F, p_i, p_f, k).reshape(-1), g[k])
