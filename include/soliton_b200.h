@@ -252,6 +252,25 @@ int ss_charge(ss_handle *h, const void *field, int which, double *out);
  * Used to hand a relaxation from FP32 to FP64 fields and back.  In place only for
  * equal element types.  No reference counterpart (the reference is FP64 only). */
 int ss_convert_field(ss_handle *h, const void *src, int src_precision, void *dst, int dst_precision, int project);
+/* Exact derivative of the discrete energy sum E_h = dA sum_s e(phi, Dx phi, Dy phi)
+ * (the reference's compute_energy_kernel summed, e.g. theories/chiral_magnet/
+ * kernels.py:125-251) with respect to every field value, divided by dA, into `out`
+ * (double, nf planes of N, true rows: dE/dpsi for the demag field, unprojected, no halo
+ * zeroing): de/dphi(t) - D1x[mask de/d(dx phi)](t) - D1y[mask de/d(dy phi)](t), the
+ * partials of the energy point by forward-mode dual numbers.  The flow's stencil
+ * gradient equals it only to O(h^4); with minus_stencil != 0 (SS_FP64 handles) `out`
+ * receives that difference (out minus ss_energy_gradient's result).  Uses the flow
+ * buffers of the bound workspace as scratch (not during a step).  No reference
+ * counterpart (the adjoint's discretisation correction). */
+int ss_energy_gradient_exact(ss_handle *h, const void *field, double *out, int minus_stencil);
+/* Add a fixed field `force` (device, double, nf planes of N in the true rows of
+ * ss_energy_gradient, 16-byte aligned; NULL removes it) to the flow's gradient rows in
+ * every stage of the following steps, before the halo zeroing and the unit-norm
+ * projection; the stage-4 err includes it.  SS_FP64 handles only.  A graph captured
+ * before the call keeps its old forcing.  With force = the residual of
+ * ss_energy_gradient_exact at a relaxed field, the flow relaxes to the stationary point
+ * of the discrete energy sum itself, to O(h^8).  No reference counterpart. */
+int ss_set_forcing(ss_handle *h, const double *force);
 /* Diagnostic density of `field` (element type of the handle) into the device array
  * `out` (double; N sites, 2 N for SS_DENSITY_SUPERCURRENT: the x plane, then the y
  * plane), asynchronous on the handle's stream; needs no workspace.  Replaces the

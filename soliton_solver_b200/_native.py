@@ -120,6 +120,8 @@ _SIG = {
     "ss_coupling_grad": ([_P, _P, _I, ctypes.POINTER(_D)], _I),
     "ss_field_density": ([_P, _P, _I, _P], _I),
     "ss_convert_field": ([_P, _P, _I, _P, _I, _I], _I),
+    "ss_energy_gradient_exact": ([_P, _P, _P, _I], _I),
+    "ss_set_forcing": ([_P, _P], _I),
     "ss_energy_noalloc": ([_I, _P, _I, _P, _I, _I, _P, ctypes.POINTER(_D), _P], _I),
     "ss_rk4_stage": ([_P, _P, _P, _P, _P, _P, _P, _D], _I),
     "ss_batch_create": ([_I, _I, _P, _I, _P, _I, _I, ctypes.POINTER(_P)], _I),

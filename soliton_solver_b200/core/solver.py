@@ -204,6 +204,29 @@ class Solver:
             nat.check(self._lib.ss_energy_gradient(self._h, _ptr(field), _ptr(out)))
         return out
 
+    def energy_gradient_exact(self, field, out=None, minus_stencil: bool = False):
+        """dE_h/dphi / dA of the discrete energy sum, exactly (true rows, unprojected;
+        see ss_energy_gradient_exact), FP64; with `minus_stencil` (FP64 solvers) minus the
+        flow's functional derivative: the O(h^4) discretisation residual.  Uses the
+        workspace's flow buffers: not during a step."""
+        self._check(field)
+        out = out if out is not None else torch.empty(self.nf * self.N, dtype=torch.float64, device=self.device)
+        self._check(out, torch.float64)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_energy_gradient_exact(self._h, _ptr(field), _ptr(out), 1 if minus_stencil else 0))
+        return out
+
+    def set_forcing(self, force=None):
+        """Add the fixed FP64 field `force` (true rows) to the flow's gradient in every
+        following step (None removes it); see ss_set_forcing.  The tensor is kept alive
+        while it is set."""
+        if force is not None:
+            self._check(force, torch.float64)
+            if force.numel() != self.nf * self.N:
+                raise ValueError("forcing must have nf * N entries")
+        nat.check(self._lib.ss_set_forcing(self._h, _ptr(force)))
+        self._force = force
+
     def energy(self, field) -> float:
         self._check(field)
         out = ctypes.c_double()

@@ -19,6 +19,7 @@
 #include "render.cuh"
 #include "init.cuh"
 #include "observe.cuh"
+#include "adjoint.cuh"
 #include "text.cuh"
 #include "theories.cuh"
 
@@ -126,6 +127,7 @@ struct ss_handle {
   long long wait_cycles = WAIT_CYCLES;
   mutable int inject_timeout = 0;  // test hook, consumed by the next flow launch
   cudaGraphExec_t graph = nullptr;  // captured n-step relaxation (ss_graph_create)
+  const double* force = nullptr;    // FP64 flows: field added to the gradient rows (ss_set_forcing)
   // page-locked host staging of ss_step: energy and err trajectories of one chunk and
   // the StepState, copied with one synchronisation (allocated on the first ss_step)
   double* host_stage = nullptr;
@@ -437,6 +439,7 @@ struct Fused {
     A.P = h->P;
     A.st = h->st;
     A.partial = h->partial;
+    A.force = h->force;
     A.E_idx = -1;
     A.err_idx = -1;
     A.prev_energy = NAN;
@@ -650,6 +653,21 @@ struct Fused {
     A.out_l = (R*)l_out;
     const bool tma = encode_tile_map(&A.tm_phi, field, sizeof(R), h->G.X, h->G.Y, TH::NF);
     return launch(h, A, tma);
+  }
+
+  // dE_h/dphi / dA of the discrete energy sum (true rows, unprojected), optionally
+  // minus the flow's functional derivative in the same rows (FP64 fields)
+  static int energy_gradient_exact(ss_handle* h, const void* field, double* out, double* q, double* sub) {
+    if (sub) {
+      int rc = Fused<TH, double>::gradient(h, field, sub, nullptr, 1);
+      if (rc) return rc;
+    }
+    exact_partials_kernel<TH, R><<<grid_1d(h->G.N), 256, 0, h->stream>>>((const R*)field, out, q, h->G, h->P);
+    CK(cudaGetLastError());
+    exact_transpose_kernel<double><<<grid_1d((long long)TH::NF * h->G.N), 256, 0, h->stream>>>(out, q, sub, TH::NF,
+                                                                                              h->G);
+    CK(cudaGetLastError());
+    return SS_OK;
   }
 
   // the observable: exact FP64 stencil of the stored values for every precision
@@ -1314,6 +1332,37 @@ int ss_convert_field(ss_handle* h, const void* src, int src_precision, void* dst
     CK(cudaGetLastError());
     return SS_OK;
   });
+}
+
+int ss_energy_gradient_exact(ss_handle* h, const void* field, double* out, int minus_stencil) {
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!field || !out) return fail(SS_ERR_ARG, "NULL argument");
+  if (h->precision == SS_PLAIN_FP64) return fail(SS_ERR_ARG, "ss_energy_gradient_exact needs SS_FP32 or SS_FP64");
+  if (minus_stencil && h->precision != SS_FP64)
+    return fail(SS_ERR_ARG, "the residual against the stencil gradient needs SS_FP64 fields");
+  const size_t nfN = (size_t)h->nf * (size_t)h->G.N;
+  const size_t q_bytes = align_up(2 * nfN * sizeof(double));
+  const size_t need = q_bytes + (minus_stencil ? nfN * sizeof(double) : 0);
+  char* region = (char*)h->l[0];
+  if (!region || region + need > h->ws + h->ws_bytes)
+    return fail(SS_ERR_WORKSPACE, "the workspace's flow buffers (%zu bytes) cannot hold the %zu bytes of scratch",
+                (size_t)(h->ws + h->ws_bytes - region), need);
+  double* q = (double*)region;
+  double* sub = minus_stencil ? (double*)(region + q_bytes) : nullptr;
+  return dispatch(h, [&](auto* tag) -> int {
+    using TH = std::remove_pointer_t<decltype(tag)>;
+    if (h->precision == SS_FP32) return Fused<TH, float>::energy_gradient_exact(h, field, out, q, sub);
+    return Fused<TH, double>::energy_gradient_exact(h, field, out, q, sub);
+  });
+}
+
+int ss_set_forcing(ss_handle* h, const double* force) {
+  if (!h) return fail(SS_ERR_ARG, "NULL handle");
+  if (force && h->precision != SS_FP64) return fail(SS_ERR_ARG, "a forcing needs SS_FP64 fields");
+  if (((uintptr_t)force) % 16) return fail(SS_ERR_ARG, "the forcing must be 16-byte aligned");
+  h->force = force;
+  return SS_OK;
 }
 
 int ss_field_density(ss_handle* h, const void* field, int kind, double* out) {

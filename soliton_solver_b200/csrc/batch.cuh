@@ -88,6 +88,7 @@ __global__ void __launch_bounds__(NT, (batch_ctas<R, MODE>()))
     const bool copy = (MODE == M_S2 || MODE == M_S23) && B.copy_out;
     A.copy_phi = copy ? (R*)I.buf[2] : nullptr;
     A.copy_vel = copy ? (R*)I.buf[3] : nullptr;
+    A.force = nullptr;
     A.partial = I.partial;
     A.st = I.st;
     A.E_traj = I.E_traj;

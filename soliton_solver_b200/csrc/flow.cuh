@@ -58,6 +58,7 @@ struct FlowArgs {
   R* vel_out;   // S4
   R* copy_phi;  // S2 / M_S23, one tile per CTA (nullable): copy of phi's and V's centres, so
   R* copy_vel;  //   that this step's S4 can read them there and write into phi / vel
+  const double* force;  // FP64 fields (nullable): added to the flow's gradient rows in every stage
   double* partial;  // per-block energy partials
   StepState* st;
   double* E_traj;   // nullable
@@ -433,6 +434,16 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
 
     V g[NF];
     TH::gradient(J, A.P, g);
+    if constexpr (sizeof(R) == 8 && MODE != M_GRAD) {
+      if (A.force) {  // uniform: a fixed field added to the flow's gradient (ss_set_forcing)
+        V fo[NF];
+#pragma unroll
+        for (int a = 0; a < NF; ++a) fo[a] = gload<V, double>(A.force + a * N + sidx, FAST, v1);
+        TH::flow_rows(fo, A.P);
+#pragma unroll
+        for (int a = 0; a < NF; ++a) g[a] = g[a] + fo[a];
+      }
+    }
     if constexpr (MODE == M_GRAD) {
       if (A.grad_raw) {
         // functional derivative of the energy: no halo zeroing, no projection, and

@@ -56,12 +56,14 @@ struct ChiralMagnet {
   // derived slots filled on the host (ChiralMagnet::derive):
   //   c[12] -2 D10  c[13] -2 D11  c[14] 2 D00  c[15] 2 D01  c[16] 2 D10  c[17] 2 D11
   //   c[18] -2 D00  c[19] -2 D01  c[20] -2 coup_K  c[21] 1/(2 coup_mu)  c[22] -1/coup_mu
+  //   c[23] -coup_mu
   static void derive(Phys& P) {
     P.c[12] = -2.0 * P.c[5]; P.c[13] = -2.0 * P.c[6]; P.c[14] = 2.0 * P.c[3]; P.c[15] = 2.0 * P.c[4];
     P.c[16] = 2.0 * P.c[5]; P.c[17] = 2.0 * P.c[6]; P.c[18] = -2.0 * P.c[3]; P.c[19] = -2.0 * P.c[4];
     P.c[20] = -2.0 * P.c[0];
     P.c[21] = P.c[2] != 0.0 ? 1.0 / (2.0 * P.c[2]) : 0.0;
     P.c[22] = P.c[2] != 0.0 ? -1.0 / P.c[2] : 0.0;
+    P.c[23] = -P.c[2];
   }
   template <typename R>
   __device__ static inline void gradient(const Jet<R, NF>& J, const Phys& P, R g[NF]) {
@@ -97,18 +99,25 @@ struct ChiralMagnet {
   __device__ static inline void true_rows(R g[NF], const Phys& P) {
     if (P.k[0]) g[3] = g[3] * pk<R>(P, 22);
   }
+  // the inverse: rows of dE/dphi as the flow stores them
+  template <typename R>
+  __device__ static inline void flow_rows(R g[NF], const Phys& P) {
+    if (P.k[0]) g[3] = g[3] * pk<R>(P, 23);
+  }
 
-  // compute_energy_point, kernels.py:125-216
-  __device__ static inline double energy(const Jet1<double, NF>& J, const Phys& P, double dA) {
+  // compute_energy_point, kernels.py:125-216.  T is double, or a dual number for the
+  // derivatives of the energy point with respect to its jet (adjoint.cuh).
+  template <typename T>
+  __device__ static inline T energy(const Jet1<T, NF>& J, const Phys& P, double dA) {
     const double cK = P.c[0], ch = P.c[1];
     const double D00 = P.c[3], D01 = P.c[4], D10 = P.c[5], D11 = P.c[6];
-    double e = 0.0;
+    T e = T(0.0);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       e += 0.5 * J.dx[a] * J.dx[a];
       e += 0.5 * J.dy[a] * J.dy[a];
     }
-    const double* m = J.f;
+    const T* m = J.f;
     // i = x
     if (D00 != 0.0) { e += D00 * m[1] * J.dx[2]; e -= D00 * m[2] * J.dx[1]; }
     if (D10 != 0.0) { e -= D10 * m[0] * J.dx[2]; e += D10 * m[2] * J.dx[0]; }
@@ -118,7 +127,7 @@ struct ChiralMagnet {
     if (D01 != 0.0) { e += D01 * m[1] * J.dy[2]; e -= D01 * m[2] * J.dy[1]; }
     if (D11 != 0.0) { e -= D11 * m[0] * J.dy[2]; e += D11 * m[2] * J.dy[0]; }
     if (P.k[0]) e -= m[3] * J.dy[1] + J.dy[3] * J.dy[3] * i2mu;
-    const double mz = m[2];
+    const T mz = m[2];
     e += ch * (1.0 - mz);
     e += cK * (1.0 - mz * mz);
     return e * dA;
@@ -186,6 +195,8 @@ struct BabySkyrme {
   static constexpr int S1_CTAS = 1;
   template <typename R>
   __device__ static inline void true_rows(R*, const Phys&) {}
+  template <typename R>
+  __device__ static inline void flow_rows(R*, const Phys&) {}
 
   template <typename S>
   __device__ static inline S spow(S a, S b) {
@@ -309,31 +320,32 @@ struct BabySkyrme {
     return u;
   }
 
-  // compute_energy_point, kernels.py:127-199
-  __device__ static inline double energy(const Jet1<double, NF>& J, const Phys& P, double dA) {
+  // compute_energy_point, kernels.py:127-199 (T: double, or a dual number, adjoint.cuh)
+  template <typename T>
+  __device__ static inline T energy(const Jet1<T, NF>& J, const Phys& P, double dA) {
     const double mpi = P.c[0], mpi2 = mpi * mpi, kappa = P.c[1], kappa2 = kappa * kappa;
-    const double gx = J.dx[0] * J.dx[0] + J.dx[1] * J.dx[1] + J.dx[2] * J.dx[2];
-    const double gy = J.dy[0] * J.dy[0] + J.dy[1] * J.dy[1] + J.dy[2] * J.dy[2];
-    double e = 0.5 * (gx + gy);
-    const double cx = J.dx[1] * J.dy[2] - J.dx[2] * J.dy[1];
-    const double cy = J.dx[2] * J.dy[0] - J.dx[0] * J.dy[2];
-    const double cz = J.dx[0] * J.dy[1] - J.dx[1] * J.dy[0];
+    const T gx = J.dx[0] * J.dx[0] + J.dx[1] * J.dx[1] + J.dx[2] * J.dx[2];
+    const T gy = J.dy[0] * J.dy[0] + J.dy[1] * J.dy[1] + J.dy[2] * J.dy[2];
+    T e = 0.5 * (gx + gy);
+    const T cx = J.dx[1] * J.dy[2] - J.dx[2] * J.dy[1];
+    const T cy = J.dx[2] * J.dy[0] - J.dx[0] * J.dy[2];
+    const T cz = J.dx[0] * J.dy[1] - J.dx[1] * J.dy[0];
     e += 0.5 * kappa2 * (cx * cx + cy * cy + cz * cz);
-    const double m1 = J.f[0], m2 = J.f[1], m3 = J.f[2];
+    const T m1 = J.f[0], m2 = J.f[1], m3 = J.f[2];
     if (P.k[0]) e += mpi2 * (1.0 - m3);
-    if (P.k[1]) { const double t = 1.0 - m3; e += mpi2 * t * t * t * t; }
+    if (P.k[1]) { const T t = 1.0 - m3; e += mpi2 * t * t * t * t; }
     if (P.k[2]) e += 0.5 * mpi2 * m1 * m1;
     if (P.k[3]) e += 0.5 * mpi2 * (1.0 - m1 * m1) * (1.0 - m3 * m3);
-    if (P.k[4]) { const double t = 1.0 - m3; e += 0.5 * mpi2 * t * (1.0 + t * t * t); }
+    if (P.k[4]) { const T t = 1.0 - m3; e += 0.5 * mpi2 * t * (1.0 + t * t * t); }
     if (P.k[5]) e += 16.0 * mpi2 * (1.0 - m3) * (1.0 + 3.0 * m3 * m3 + 3.0 * m1 * m2 * m2 - m1 * m1 * m1);
     if (P.k[6]) {
-      double zr = m1, zi = m2;
+      T zr = m1, zi = m2;
       for (int i = 0; i < P.k[8] - 1; ++i) {
-        const double tr = zr * m1 - zi * m2;
+        const T tr = zr * m1 - zi * m2;
         zi = zr * m2 + zi * m1;
         zr = tr;
       }
-      const double wr = 1.0 - zr, wi = -zi;
+      const T wr = 1.0 - zr, wi = -zi;
       e += mpi2 * (1.0 - m3) * (wr * wr + wi * wi);
     }
     if (P.k[7]) e += mpi2 * (1.0 - m3 * m3);
@@ -411,6 +423,8 @@ struct GinzburgLandau {
   static constexpr int S1_CTAS = 1;
   template <typename R>
   __device__ static inline void true_rows(R*, const Phys&) {}
+  template <typename R>
+  __device__ static inline void flow_rows(R*, const Phys&) {}
 
   // derived slot: c[4] Lambda / 2
   static void derive(Phys& P) { P.c[4] = 0.5 * P.c[1]; }
@@ -435,20 +449,22 @@ struct GinzburgLandau {
            q * q * Asq * psi2 - pot * psi2;
   }
 
-  // compute_energy_point, kernels.py:46-108 (u read from p_f[9] as the reference does)
-  __device__ static inline double energy(const Jet1<double, NF>& J, const Phys& P, double dA) {
+  // compute_energy_point, kernels.py:46-108 (u read from p_f[9] as the reference does;
+  // T: double, or a dual number, adjoint.cuh)
+  template <typename T>
+  __device__ static inline T energy(const Jet1<T, NF>& J, const Phys& P, double dA) {
     const double q = P.c[0], lam = P.c[1], u1 = P.c[3];
-    const double A1 = J.f[0], A2 = J.f[1], psi1 = J.f[2], psi2 = J.f[3];
-    const double dpsi1dx = J.dx[2], dpsi1dy = J.dy[2], dpsi2dx = J.dx[3], dpsi2dy = J.dy[3];
-    const double psi_sq = psi1 * psi1 + psi2 * psi2;
-    const double A_sq = A1 * A1 + A2 * A2;
-    double e = 0.0;
+    const T A1 = J.f[0], A2 = J.f[1], psi1 = J.f[2], psi2 = J.f[3];
+    const T dpsi1dx = J.dx[2], dpsi1dy = J.dy[2], dpsi2dx = J.dx[3], dpsi2dy = J.dy[3];
+    const T psi_sq = psi1 * psi1 + psi2 * psi2;
+    const T A_sq = A1 * A1 + A2 * A2;
+    T e = T(0.0);
     e += 0.5 * (dpsi1dx * dpsi1dx + dpsi1dy * dpsi1dy + dpsi2dx * dpsi2dx + dpsi2dy * dpsi2dy);
     e += q * A1 * (psi1 * dpsi2dx - psi2 * dpsi1dx);
     e += q * A2 * (psi1 * dpsi2dy - psi2 * dpsi1dy);
     e += 0.5 * q * q * A_sq * psi_sq;
     e += lam / 8.0 * (u1 * u1 - psi_sq) * (u1 * u1 - psi_sq);
-    const double curlA = J.dx[1] - J.dy[0];
+    const T curlA = J.dx[1] - J.dy[0];
     e += 0.5 * curlA * curlA;
     return e * dA;
   }
@@ -505,6 +521,8 @@ struct Anisotropic {
   static constexpr int S1_CTAS = 1;
   template <typename R>
   __device__ static inline void true_rows(R*, const Phys&) {}
+  template <typename R>
+  __device__ static inline void flow_rows(R*, const Phys&) {}
 
   template <typename R>
   __device__ static inline R gamR(int i, int a, int b, const Phys& P) {
@@ -585,27 +603,28 @@ struct Anisotropic {
     for (int a = 0; a < 6; ++a) g[a] = EG[a];
   }
 
-  // compute_energy_point, kernels.py:97-170
-  __device__ static inline double energy(const Jet1<double, NF>& J, const Phys& P, double dA) {
+  // compute_energy_point, kernels.py:97-170 (T: double, or a dual number, adjoint.cuh)
+  template <typename T>
+  __device__ static inline T energy(const Jet1<T, NF>& J, const Phys& P, double dA) {
     const double kappa = P.c[0], Q = P.c[1], a1 = P.c[2], a2 = P.c[3];
     const double b1 = P.c[4], b2 = P.c[5], b3 = P.c[6], b4 = P.c[7];
-    const double A[2] = {J.f[0], J.f[1]};
-    const double p1r = J.f[2], p1i = J.f[3], p2r = J.f[4], p2i = J.f[5];
-    const double p1sq = p1r * p1r + p1i * p1i, p2sq = p2r * p2r + p2i * p2i;
-    const double curl = J.dx[1] - J.dy[0];
-    const double F_mag = 0.5 * kappa * kappa * (curl * curl);
-    double F_pot = 0.0;
+    const T A[2] = {J.f[0], J.f[1]};
+    const T p1r = J.f[2], p1i = J.f[3], p2r = J.f[4], p2i = J.f[5];
+    const T p1sq = p1r * p1r + p1i * p1i, p2sq = p2r * p2r + p2i * p2i;
+    const T curl = J.dx[1] - J.dy[0];
+    const T F_mag = 0.5 * kappa * kappa * (curl * curl);
+    T F_pot = T(0.0);
     F_pot += a1 * p1sq + a2 * p2sq;
     F_pot += b1 * p1sq * p1sq + b2 * p2sq * p2sq + b3 * p1sq * p2sq;
     F_pot += 2.0 * b4 * (p1r * p1r * p2r * p2r + p1i * p1i * p2i * p2i - p1i * p1i * p2r * p2r -
                          p1r * p1r * p2i * p2i + 4.0 * p1r * p1i * p2r * p2i);
-    double F_kin = 0.0;
+    T F_kin = T(0.0);
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
-      const double Ai = A[i];
-      const double* d = (i == 0) ? J.dx : J.dy;
+      const T Ai = A[i];
+      const T* d = (i == 0) ? J.dx : J.dy;
       const double g00 = gam(i, 0, 0, P), g01 = gam(i, 0, 1, P), g10 = gam(i, 1, 0, P), g11 = gam(i, 1, 1, P);
-      const double r1 = d[2], i1 = d[3], r2 = d[4], i2 = d[5];
+      const T r1 = d[2], i1 = d[3], r2 = d[4], i2 = d[5];
       F_kin += 0.5 * g00 * (r1 * r1 + i1 * i1 + Q * Ai * (p1r * i1 - p1i * r1) + Q * Ai * (p1r * i1 - p1i * r1) +
                             Q * Q * Ai * Ai * p1sq);
       F_kin += 0.5 * g01 * (r1 * r2 + i1 * i2 + Q * Ai * (p1r * i2 - p1i * r2) + Q * Ai * (p2r * i1 - p2i * r1) +
@@ -615,7 +634,7 @@ struct Anisotropic {
       F_kin += 0.5 * g11 * (r2 * r2 + i2 * i2 + Q * Ai * (p2r * i2 - p2i * r2) + Q * Ai * (p2r * i2 - p2i * r2) +
                             Q * Q * Ai * Ai * p2sq);
     }
-    double e = F_kin + F_mag + F_pot;
+    T e = F_kin + F_mag + F_pot;
     e -= P.c[11];
     return e * dA;
   }
