@@ -415,6 +415,65 @@ def relaxed_accuracy(dev, tol=1e-6, plain_steps=20_000):
     return out
 
 
+def c5_workflow(dev, tol=1e-5, max_steps=800_000, rel_delta=1e-2, fd_steps=400_000):
+    """The large chiral magnet end to end: the workload's 4096^2 lattice (64 anti-skyrmions,
+    B = 0.2 T, Heusler, demag on) relaxed by Simulation.minimize(tol) (FP32 arrested flow
+    to its energy plateau, then FP64 on the projected state), its topological charge, and
+    dE_min/dB, dE_min/dD from the discretisation-consistent adjoint
+    (relaxed_coupling_gradients) against central differences of relaxed energies at
+    c (1 +- rel_delta), each relaxed by the same minimize from the relaxed state
+    (fd_steps steps at most).  The undamped RK4 dynamics is unstable for this saddle
+    system (see the module docstring), so the first 2000 steps are steps of the arrested
+    flow too.  Central-difference truncation at rel_delta = 1e-2: ~1e-5 relative."""
+    import torch
+    from soliton_solver_b200.autograd import coupling_gradients, relaxed_coupling_gradients
+    from soliton_solver_b200.core.simulation import Simulation
+    from soliton_solver_b200.initial_conditions import skyrmion_lattice
+    th, p = chiral_params()
+    out = {"config": config({"tol": tol, "rel_delta": rel_delta})}
+    sim = Simulation(p, th, precision="fp32", device=dev)
+    sim.load_field(skyrmion_lattice(sim.rp, n=8, R=1.0, seed=1000, device=dev))
+    out["Q0"] = sim.observables()["skyrmion_number"]
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    res = sim.minimize(tol=tol, max_steps=max_steps)
+    out["relax_wall_s"] = time.perf_counter() - t0
+    out["relax"] = {k: v for k, v in res.items() if k not in ("trajectory",)}
+    obs = sim.observables()
+    out["Q"] = obs["skyrmion_number"]
+    out["Q_dev_from_integer"] = abs(obs["skyrmion_number"] - round(obs["skyrmion_number"]))
+    out["energy"] = res["energy"]
+    t0 = time.perf_counter()
+    g_plain = coupling_gradients(sim, names=("B", "D"))  # envelope at the FP32 buffers (rounded)
+    g, info = relaxed_coupling_gradients(sim, names=("B", "D"))
+    out["adjoint_wall_s"] = time.perf_counter() - t0
+    out["adjoint"] = g
+    out["adjoint_info"] = {k: v for k, v in info.items()}
+    out["envelope_fp32_state"] = g_plain
+    F64 = sim.Field64.clone()
+    fd = {}
+    t0 = time.perf_counter()
+    for name in ("B", "D"):
+        c = getattr(p, name)
+        d = rel_delta * c
+        Es = []
+        for sgn in (1, -1):
+            ps = p.with_(**{name: c + sgn * d})
+            s2 = Simulation(ps, th, precision="fp32", device=dev)
+            s2.load_field(F64)
+            r2 = s2.minimize(tol=tol, max_steps=fd_steps)
+            Es.append((r2["energy"], r2["steps"], r2["converged"]))
+            del s2
+            torch.cuda.empty_cache()
+        fd[name] = {"fd": (Es[0][0] - Es[1][0]) / (2 * d), "steps": [Es[0][1], Es[1][1]], "delta": d,
+                    "converged": [Es[0][2], Es[1][2]]}
+        fd[name]["rel_err_adjoint"] = abs(g[name] - fd[name]["fd"]) / abs(fd[name]["fd"])
+        fd[name]["rel_err_uncorrected"] = abs(info["uncorrected"][name] - fd[name]["fd"]) / abs(fd[name]["fd"])
+    out["fd_wall_s"] = time.perf_counter() - t0
+    out["finite_differences"] = fd
+    return out
+
+
 def reference_numba_gpu(n=4096, steps=5, timeout=900):
     """The reference's own Simulation.step on Numba's real CUDA target (its FP64 kernels,
     host-side arrest), on the workload's n x n lattice, in a process of its own."""
@@ -430,12 +489,16 @@ def reference_numba_gpu(n=4096, steps=5, timeout=900):
     return res
 
 
-def batched_sweep(dev, steps=20, seed=4):
+def batched_sweep(dev, steps=20, seed=4, reps=3):
     """The batched baby Skyrme sweep: 256 lattices with edges from {64, 128, 256, 512},
     kappa, mpi ~ U(0.5, 2), windings B in 1..4, hedgehogs with R ~ U(1, 3), FP32 fields.
     Lattice spacing 0.1 and dt = 0.002: a winding-4 hedgehog with R = 1 and kappa = 2 has
     |grad m| ~ 13, so the Skyrme term's stiffness bounds the explicit step near h/26.
-    Returns point-updates/s of ss_batch_step over `steps` steps (all lattices)."""
+    `steps` steps of every lattice are captured as one CUDA graph (ss_batch_graph_create:
+    per step one launch per RK stage over all lattices' tiles, per-lattice energies and
+    arrest on the device) and replayed `reps` times between CUDA events; the same steps
+    issued by ss_batch_step (stream launches plus its per-call host copies) are timed
+    beside it.  Roofline: 14 words x 3 components x 4 bytes per point-update."""
     import torch
     from soliton_solver_b200.core.batch import BatchSolver
     from soliton_solver_b200.initial_conditions import hedgehog
@@ -451,15 +514,34 @@ def batched_sweep(dev, steps=20, seed=4):
         b.load(i, hedgehog(p.resolved(), charge=int(rng.integers(1, 5)), R=float(rng.uniform(1, 3)), seed=i,
                            device=dev))
     b.step(3, 1e300)
+    sites = int(sum(int(e) * int(e) for e in edges))
     torch.cuda.synchronize(dev)
     t = time.perf_counter()
     E, _ = b.step(steps)
     torch.cuda.synchronize(dev)
-    dt = time.perf_counter() - t
-    sites = int(sum(int(e) * int(e) for e in edges))
-    return {"lattices": 256, "sites": sites, "steps": steps, "value": sites * steps / dt / 1e6, "unit": UNIT,
-            "ms_per_step": dt / steps * 1e3, "tma": b.tma_enabled, "finite": bool(np.isfinite(E).all()),
-            "note": "ss_batch_step: one launch per RK stage over all 256 lattices, wall clock incl. host sync"}
+    dt_stream = time.perf_counter() - t
+    b.capture(steps)
+    b.replay()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(reps):
+        b.replay()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / (reps * steps)
+    Eg, _ = b.trajectory()
+    peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0)) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    gbs = sites * 14 * 3 * 4 / (ms / 1e3) / 1e9
+    return {"lattices": 256, "sites": sites, "steps_per_graph": steps, "replays": reps,
+            "value": sites / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms,
+            "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak, "bytes_per_point_update": 168,
+            "stream_value": sites * steps / dt_stream / 1e6, "stream_ms_per_step": dt_stream / steps * 1e3,
+            "tma": b.tma_enabled, "finite": bool(np.isfinite(E).all() and np.isfinite(Eg).all()),
+            "note": "one CUDA-graph launch per `steps` steps of all 256 lattices, CUDA events around the replays; "
+                    "stream_value: ss_batch_step incl. its host synchronisation"}
 
 
 def small_lattice_graph(dev, steps=2000, chunk=100):
@@ -685,6 +767,9 @@ def main():
                                                     "(comma-separated, 0 one tile per CTA, 1 pipelined)")
     ap.add_argument("--size", type=int, default=4096, help="lattice edge (4096 is the workload; smaller sizes "
                                                              "are for profiler captures)")
+    ap.add_argument("--workflow", default="", choices=["", "c5"],
+                    help="c5: relax the workload's lattice to tol and check dE/dB, dE/dD against finite "
+                         "differences (minutes of GPU time; prints one JSON line)")
     args = ap.parse_args()
     global XLEN, YLEN, XSIZE
     if args.size != 4096:
@@ -696,6 +781,12 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.workflow == "c5":
+        import torch
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        print(json.dumps(c5_workflow(dev), default=float), flush=True)
+        return 0
     if world > 1:
         import datetime
         import torch

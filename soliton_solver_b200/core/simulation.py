@@ -151,8 +151,9 @@ class Simulation:
                        run at about a third of the FP64 cost; FP32 rounding bounds how far
                        they get (the gradient stalls at ~eps/h^2), and the FP64 steps
                        finish from there.
-        A phase reaches its plateau when its energy falls by less than ``plateau`` x |E|
-        over two chunks in a row.  ``max_steps`` bounds the total.  Needs the arrested
+        A phase reaches its plateau when its energy moves by less than ``plateau`` x |E|
+        over two chunks in a row (in either direction: the flow of a saddle field such as
+        the chiral magnet's demag potential raises E while it converges).  ``max_steps`` bounds the total.  Needs the arrested
         flow (killkinen on).
 
         Returns a dict: energy (FP64 observable of the final field), err, converged,
@@ -210,7 +211,7 @@ class Simulation:
                     break
                 steps += n
                 E, err = float(Eh[-1]), float(rh[-1])
-                hits = hits + 1 if E_prev - E < plateau * abs(E) else 0
+                hits = hits + 1 if abs(E_prev - E) < plateau * abs(E) else 0
                 E_prev = E
                 if hits >= 2 and prec == "fp32":
                     stop = "plateau"

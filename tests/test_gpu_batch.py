@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 import torch
 
+from oracle import flow64 as ref
 from soliton_solver_b200.core.batch import BatchSolver
 from soliton_solver_b200.core.solver import Solver
 from soliton_solver_b200.theories import load_theory
@@ -131,10 +132,41 @@ def test_batch_trajectories_across_chunks():
         np.testing.assert_allclose(b.fields[i].cpu().numpy(), f.cpu().numpy(), rtol=0, atol=1e-11)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_trajectories_vs_oracle(precision):
+    """Each lattice of a batch against the FP64 oracle's own arrested-Newton steps from the
+    same field (not through the single-lattice solver): FP64 energies 1e-12 relative and
+    fields 1e-12; FP32 (oracle on the FP32-rounded field) energies 1e-6, fields 1e-5."""
+    th = load_theory("Baby Skyrme")
+    sizes = [(64, 64), (40, 200), (33, 70)]
+    rng = np.random.default_rng(21)
+    params = [th.params.default_params(xlen=X, ylen=Y, lsx=0.1, lsy=0.1, time_step=0.02,
+                                       kappa=float(rng.uniform(0.5, 2)), mpi=float(rng.uniform(0.5, 2)),
+                                       unit_magnetization=True) for X, Y in sizes]
+    fields = [_hedgehog(p.resolved(), B=i + 1, R=float(rng.uniform(1, 3)), seed=i) for i, p in enumerate(params)]
+    if precision == "fp32":
+        fields = [F.astype(np.float32).astype(np.float64) for F in fields]
+    b = BatchSolver(th, params, precision)
+    for i, F in enumerate(fields):
+        b.load(i, F)
+    prev = np.full(len(sizes), 1e300)
+    prev[2] = -1e300  # arrest fires for this lattice
+    n = 5
+    E, err = b.step(n, prev)
+    tol_E, tol_F = (1e-12, 1e-12) if precision == "fp64" else (1e-6, 1e-5)
+    for i, p in enumerate(params):
+        p_i, p_f = th.params.pack_device_params(p.resolved())
+        Fo, _, Ew, errw = ref.relax("baby_skyrme", fields[i], np.zeros_like(fields[i]), float(prev[i]), p_i, p_f, n)
+        np.testing.assert_allclose(E[i], Ew, rtol=tol_E)
+        assert float(np.max(np.abs(b.fields[i].double().cpu().numpy() - Fo.reshape(-1)))) <= tol_F
+        np.testing.assert_allclose(err[i], errw, rtol=1e-4 if precision == "fp32" else 1e-10)
+
+
 def test_batch_sweep_config_shape():
     """256 lattices with sizes from {64, 128, 256, 512}^2, random couplings and charges
-    (the batched baby Skyrme sweep), FP32: runs and keeps every energy finite and each
-    lattice's charge near its winding."""
+    (the batched baby Skyrme sweep), FP32: runs and keeps every energy finite, and three
+    sampled lattices (one of each of the three smaller sizes) follow the FP64 oracle's
+    steps from the same FP32 field (energies 1e-6 relative)."""
     th = load_theory("Baby Skyrme")
     rng = np.random.default_rng(4)
     edges = rng.choice([64, 128, 256, 512], size=256)
@@ -145,8 +177,14 @@ def test_batch_sweep_config_shape():
     assert b.tma_enabled
     for i, p in enumerate(params):
         b.load(i, _hedgehog(p.resolved(), B=1, R=1.5, seed=i))
+    F0 = [f.double().cpu().numpy() for f in b.fields]
     E, err = b.step(20, 1e300)
     assert np.all(np.isfinite(E)) and E.shape == (256, 20)
+    for e in (64, 128, 256):
+        i = int(np.nonzero(edges == e)[0][0])
+        p_i, p_f = th.params.pack_device_params(params[i].resolved())
+        _, _, Ew, _ = ref.relax("baby_skyrme", ref.as_field(F0[i], p_i), np.zeros((3, e, e)), 1e300, p_i, p_f, 3)
+        np.testing.assert_allclose(E[i, :3], Ew, rtol=1e-6)
 
 
 def test_graph_replay_equals_stream_steps():

@@ -1,8 +1,15 @@
 """The headline lattice at full size: chiral magnet 4096 x 4096, FP32 fields, Heusler DMI,
-demag on, B = 0.2 T, 64 anti-skyrmions on a jittered lattice, killkinen off.
+demag on, B = 0.2 T, 64 anti-skyrmions on a jittered lattice, arrested Newton flow.
 
-The oracle cannot run a 16.8 M-site step in a test's time, so full-size parity rests
-on properties that do not depend on the size:
+  * whole lattice: one full FP32 step of the 16.8 M-site lattice against the FP64
+    oracle's step of the same (FP32-rounded) field, computed over 16 stripes of 256
+    rows with 12 rows of overlap on each cut side (a step's result at a row depends on
+    the rows within 4 stages x 2 cells, and the cut's masks reach 2 more): every site
+    of the new field to 1e-5 absolute (the FP32 trajectory tolerance of the parity
+    tests), the stage-4 err to 1e-4 x its scale, and the step's flow energy against
+    the oracle's FP64 energy of its new field to 1e-6 relative.
+
+Size-independent properties besides:
 
   * locality: the gradient at a site depends on its 5 x 5 neighbourhood only, so the
     full-lattice gradient on windows deep inside the lattice must equal the oracle's
@@ -31,7 +38,7 @@ pytestmark = pytest.mark.gpu
 X = Y = 4096
 XSIZE = 128.0
 PHYS = dict(J=40e-12, K=0.8e6, D=4e-3, M=580e3, B=0.2, dmi_term="Heusler", demag=True, unit_magnetization=True,
-            killkinen=False)
+            killkinen=True)
 
 
 def _params(th, xlen, ylen, **kw):
@@ -139,3 +146,50 @@ def test_fullsize_gradient_corners_vs_oracle(full):
             # the halo ring of the lattice edge is zeroed
             edge_x = got[:, :2, :] if lo_x else got[:, -2:, :]
             assert not np.any(edge_x)
+
+
+def _oracle_step_window(args):
+    """One oracle RK4 step of a window; returns the new field and the stage-4 gradient."""
+    win, p_i, p_f = args
+    V = np.zeros_like(win)
+    k1, T = ref.rk4_stage(V, V, win, win, 0.0, p_f)
+    l1, _ = ref.gradient_step("chiral_magnet", T, p_i, p_f)
+    k2, T = ref.rk4_stage(V, l1, win, k1, 0.5, p_f)
+    l2, _ = ref.gradient_step("chiral_magnet", T, p_i, p_f)
+    k3, T = ref.rk4_stage(V, l2, win, k2, 0.5, p_f)
+    l3, _ = ref.gradient_step("chiral_magnet", T, p_i, p_f)
+    k4, T = ref.rk4_stage(V, l3, win, k3, 1.0, p_f)
+    l4, EG = ref.gradient_step("chiral_magnet", T, p_i, p_f)
+    _, Fn = ref.rk4_finalize("chiral_magnet", V, win, k1, k2, k3, k4, l1, l2, l3, l4, p_i)
+    return Fn, EG
+
+
+def test_fullsize_whole_lattice_step_vs_oracle(full):
+    import concurrent.futures as cf
+    th, p, sim, F0 = full
+    sim.load_field(F0)
+    E, err = sim.relax(1, 1e300)
+    got = sim.Field.cpu().numpy().astype(np.float64).reshape(4, X, Y)
+    Fin = F0.cpu().numpy().astype(np.float64).reshape(4, X, Y)
+    rp = sim.rp
+    S, H = 256, 12
+    jobs, spans = [], []
+    for x0 in range(0, X, S):
+        x1 = x0 + S
+        lo, hi = max(0, x0 - H), min(X, x1 + H)
+        pw = _params(th, hi - lo, Y, lsx=rp.lsx, lsy=rp.lsy, time_step=rp.time_step, xsize=rp.lsx * (hi - lo - 1),
+                     ysize=rp.lsy * (Y - 1))
+        p_i, p_f = th.params.pack_device_params(pw.resolved())
+        jobs.append((np.ascontiguousarray(Fin[:, lo:hi, :]), p_i, p_f))
+        spans.append((x0, x1, lo))
+    want = np.empty_like(Fin)
+    err_want = -np.inf
+    with cf.ThreadPoolExecutor(8) as ex:
+        for (x0, x1, lo), (Fn, EG) in zip(spans, ex.map(_oracle_step_window, jobs)):
+            want[:, x0:x1, :] = Fn[:, x0 - lo:x1 - lo, :]
+            err_want = max(err_want, float(EG[:, x0 - lo:x1 - lo, :].max()))
+    assert float(np.max(np.abs(got - want))) <= 1e-5
+    assert abs(float(err[0]) - err_want) <= 1e-4 * max(abs(err_want), 1.0)
+    p_i, p_f = th.params.pack_device_params(rp)
+    E_want = ref.energy("chiral_magnet", want, p_i, p_f)
+    assert abs(float(E[0]) - E_want) <= 1e-6 * abs(E_want)
