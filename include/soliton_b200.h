@@ -333,6 +333,19 @@ int ss_batch_bind(ss_batch *b, void *const *fields, void *const *velocities, voi
  * page-locks a host staging buffer of 16 KB per lattice, held until ss_batch_destroy. */
 int ss_batch_step(ss_batch *b, int n_steps, const double *prev_energy, double *energy_traj, double *err_traj);
 int ss_batch_tma_enabled(const ss_batch *b);
+/* Tile shapes of the batched stage kernels, chosen per size class of lattices (the
+ * lattices of equal extents): shape 0 tiles 16 x 64 sites per 256-thread CTA (three
+ * resident per SM), shape 1 tiles 8 x 32 per 128-thread CTA (six per SM; TMA-staged
+ * FP32 batches only).  ss_batch_autotune times one step's stage launches of each size
+ * class in each shape (`iters` steps, after one warm-up; only workspace scratch is
+ * written) and keeps the faster; ms_out (nullable, 2 n floats) receives, per lattice,
+ * its class's step time in shape 0 and 1 (zeros when only shape 0 applies).  Lattices
+ * of different shapes are launched as one kernel per shape and stage.  Results do not
+ * depend on the shape up to the order of the per-tile energy partials.  No reference
+ * counterpart. */
+int ss_batch_autotune(ss_batch *b, int iters, float *ms_out);
+int ss_batch_get_shape(const ss_batch *b, int lattice);
+int ss_batch_set_shape(ss_batch *b, int lattice, int shape);
 
 /* ---- CUDA graphs ---------------------------------------------------------------
  * ss_graph_create captures n_steps of ss_step_async(h, n_steps, NaN, ...) — every

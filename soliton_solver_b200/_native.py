@@ -130,6 +130,9 @@ _SIG = {
     "ss_batch_bind": ([_P, _P, _P, _P, ctypes.c_size_t, _P], _I),
     "ss_batch_step": ([_P, _I, _P, _P, _P], _I),
     "ss_batch_tma_enabled": ([_P], _I),
+    "ss_batch_autotune": ([_P, _I, _P], _I),
+    "ss_batch_get_shape": ([_P, _I], _I),
+    "ss_batch_set_shape": ([_P, _I, _I], _I),
     "ss_graph_create": ([_P, _I, _P, _P], _I),
     "ss_graph_launch": ([_P], _I),
     "ss_batch_graph_create": ([_P, _I], _I),

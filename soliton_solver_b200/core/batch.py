@@ -50,6 +50,26 @@ class BatchSolver:
     def tma_enabled(self) -> bool:
         return bool(self._lib.ss_batch_tma_enabled(self._h))
 
+    def autotune(self, iters: int = 3):
+        """Pick the tile shape of every size class (lattices of equal extents) by timing
+        one step's stage launches in each shape (see ss_batch_autotune).  Returns
+        {(xlen, ylen): (ms in 16 x 64 tiles, ms in 8 x 32 tiles, chosen shape)}."""
+        ms = np.zeros(2 * self.n, dtype=np.float32)
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_batch_autotune(self._h, int(iters), ms.ctypes.data))
+        out = {}
+        for i, rp in enumerate(self.rps):
+            out[(int(rp.xlen), int(rp.ylen))] = (float(ms[2 * i]), float(ms[2 * i + 1]), self.shape(i))
+        return out
+
+    def shape(self, i: int) -> int:
+        """Tile shape of lattice i: 0 (16 x 64 sites) or 1 (8 x 32)."""
+        return int(self._lib.ss_batch_get_shape(self._h, int(i)))
+
+    def set_shape(self, i: int, shape: int):
+        with torch.cuda.device(self.device):
+            nat.check(self._lib.ss_batch_set_shape(self._h, int(i), int(shape)))
+
     def load(self, i: int, field, velocity=None):
         f = torch.as_tensor(np.asarray(field) if not isinstance(field, torch.Tensor) else field)
         self.fields[i].copy_(f.reshape(-1).to(self.dtype))

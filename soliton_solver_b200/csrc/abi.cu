@@ -67,13 +67,14 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // 3-D map over component planes (dims y, x, component) whose box is one staged
 // tile: (TY + 8) x (TX + 4) x NF.  Fails (-> plain loads) when the buffer or its
 // row pitch is not 16-byte aligned.
-bool encode_tile_map(CUtensorMap* m, const void* ptr, size_t es, int X, int Y, int NF, bool centre = false) {
+bool encode_tile_map(CUtensorMap* m, const void* ptr, size_t es, int X, int Y, int NF, bool centre = false,
+                     int tx = TX, int ty = TY) {
   if (!ptr || ((uintptr_t)ptr) % 16 || ((size_t)Y * es) % 16) return false;
   auto fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[3] = {(cuuint64_t)Y, (cuuint64_t)X, (cuuint64_t)NF};
   cuuint64_t strides[2] = {(cuuint64_t)Y * es, (cuuint64_t)X * Y * es};
-  cuuint32_t box[3] = {(cuuint32_t)(centre ? TY : TY + 8), (cuuint32_t)(centre ? TX : TX + 4), (cuuint32_t)NF};
+  cuuint32_t box[3] = {(cuuint32_t)(centre ? ty : ty + 8), (cuuint32_t)(centre ? tx : tx + 4), (cuuint32_t)NF};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(m, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
                   const_cast<void*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -1504,17 +1505,28 @@ extern "C" int ss_energy_noalloc(int theory, const int32_t* p_i, int n_i, const 
 // ===========================================================================
 // Batched lattices: many independent relaxations of one theory per launch
 // ===========================================================================
+// Tile shapes of the batched stage kernels (x rows, y columns, threads): the
+// autotuner picks one per size class of lattices (ss_batch_autotune).  Shape 1 exists
+// for TMA-staged FP32 batches.
+constexpr int N_BATCH_SHAPES = 2;
+constexpr int BSHAPE_TX[N_BATCH_SHAPES] = {16, 8};
+constexpr int BSHAPE_TY[N_BATCH_SHAPES] = {64, 32};
+
 struct ss_batch {
   int theory = 0, precision = 0, n = 0, nf = 0;
   size_t elem = 4;
   std::vector<ss_handle> inst;   // decoded parameters per lattice (host only)
-  std::vector<int> tiles;        // tiles per lattice
-  int total_tiles = 0;
+  std::vector<int> shape;        // tile shape per lattice
+  std::vector<int> max_tiles;    // tiles per lattice in its finest shape (partials are sized for it)
+  int total_max = 0;             // sum of max_tiles: capacity of each tile list
+  int group_tiles[N_BATCH_SHAPES] = {0, 0};  // tiles of the lattices of each shape
   bool tma = false;
   cudaStream_t stream = nullptr;
   char* ws = nullptr;
   BatchInst* d_insts = nullptr;
-  int* d_tile_inst = nullptr;
+  int* d_tile_inst[N_BATCH_SHAPES] = {nullptr, nullptr};  // lattice of each tile, per shape group
+  int* d_tune_tiles = nullptr;   // a single size class's tiles while the autotuner times it
+  float tune_ms[64][N_BATCH_SHAPES] = {};  // autotuner: per size class (first 64) and shape
   double* d_prev = nullptr;
   std::vector<BatchInst> h_insts;
   std::vector<void*> fields, vels;
@@ -1542,7 +1554,8 @@ size_t batch_layout(ss_batch* b, char* base) {
     return p;
   };
   b->d_insts = (BatchInst*)take(sizeof(BatchInst) * b->n);
-  b->d_tile_inst = (int*)take(sizeof(int) * b->total_tiles);
+  for (int g = 0; g < N_BATCH_SHAPES; ++g) b->d_tile_inst[g] = (int*)take(sizeof(int) * b->total_max);
+  b->d_tune_tiles = (int*)take(sizeof(int) * b->total_max);
   b->d_prev = (double*)take(sizeof(double) * b->n);
   b->d_st = (StepState*)take(sizeof(StepState) * b->n);
   b->d_E = (double*)take(sizeof(double) * TRAJ_CAP * b->n);
@@ -1552,7 +1565,7 @@ size_t batch_layout(ss_batch* b, char* base) {
     BatchInst& I = b->h_insts[i];
     const size_t fb = b->elem * (size_t)b->nf * (size_t)b->inst[i].G.N;
     I.st = b->d_st ? b->d_st + i : nullptr;
-    I.partial = (double*)take(sizeof(double) * b->tiles[i]);
+    I.partial = (double*)take(sizeof(double) * b->max_tiles[i]);
     I.E_traj = b->d_E ? b->d_E + (size_t)i * TRAJ_CAP : nullptr;
     I.err_traj = b->d_err ? b->d_err + (size_t)i * TRAJ_CAP : nullptr;
     for (int k = 2; k < 7; ++k) I.buf[k] = take(fb);
@@ -1562,22 +1575,36 @@ size_t batch_layout(ss_batch* b, char* base) {
 
 template <class TH, typename R>
 struct Batched {
-  static constexpr size_t BUF = tile_buf_bytes<R, TH::NF, TX, TY>();
-  static inline unsigned long long smem_done[2][N_FLOW_MODES] = {};
-
-  template <bool TMA_, int MODE>
-  static int launch_mode(const ss_batch* b, const BatchStep& B) {
+  // one launch over the tiles of `tile_inst` (lattices of one tile shape)
+  template <int BTX, int BTY, int BNT, bool TMA_, int MODE>
+  static int launch_shape(const ss_batch* b, const BatchStep& B, const int* tile_inst, int ntiles) {
+    if (ntiles <= 0) return SS_OK;
+    constexpr size_t BUF = tile_buf_bytes<R, TH::NF, BTX, BTY>();
     constexpr size_t smem = TMA_ ? flow_buffers(MODE) * BUF : BUF;
-    constexpr int NTM = smem > 113 * 1024 ? 2 * NT : NT;  // as Fused::flow_threads
-    auto k = batch_flow_kernel<TH, R, TX, TY, NTM, TMA_, MODE>;
-    set_smem(k, smem, smem_done[TMA_ ? 1 : 0][MODE]);
-    k<<<b->total_tiles, NTM, smem, b->stream>>>(b->d_insts, b->d_tile_inst, B);
+    constexpr int NTM = smem > 113 * 1024 ? 2 * BNT : BNT;  // as Fused::flow_threads
+    auto k = batch_flow_kernel<TH, R, BTX, BTY, NTM, TMA_, MODE>;
+    static unsigned long long smem_done = 0;  // one per instantiation
+    set_smem(k, smem, smem_done);
+    k<<<ntiles, NTM, smem, b->stream>>>(b->d_insts, tile_inst, B);
     CK(cudaGetLastError());
     return SS_OK;
   }
+  // a stage over every shape group (shape 1: TMA-staged FP32 batches only)
   template <int MODE>
   static int launch(const ss_batch* b, const BatchStep& B) {
-    return b->tma ? launch_mode<true, MODE>(b, B) : launch_mode<false, MODE>(b, B);
+    int rc;
+    if constexpr (MODE == M_S23) {  // needs TMA staging
+      rc = launch_shape<16, 64, NT, true, MODE>(b, B, b->d_tile_inst[0], b->group_tiles[0]);
+    } else {
+      rc = b->tma ? launch_shape<16, 64, NT, true, MODE>(b, B, b->d_tile_inst[0], b->group_tiles[0])
+                  : launch_shape<16, 64, NT, false, MODE>(b, B, b->d_tile_inst[0], b->group_tiles[0]);
+    }
+    if (rc) return rc;
+    if constexpr (sizeof(R) == 4) {
+      if (b->tma && b->group_tiles[1] > 0)
+        rc = launch_shape<8, 32, 128, true, MODE>(b, B, b->d_tile_inst[1], b->group_tiles[1]);
+    }
+    return rc;
   }
 
   static int step(ss_batch* b, int n, bool use_prev) {
@@ -1604,7 +1631,7 @@ struct Batched {
       B.E_idx = -1;
       B.copy_out = land;
       if (b->tma) {  // stages 2 and 3 fused (one staging of phi, V, l1)
-        if ((rc = launch_mode<true, M_S23>(b, B))) return rc;
+        if ((rc = launch<M_S23>(b, B))) return rc;
       } else {
         if ((rc = launch<M_S2>(b, B))) return rc;
         B.copy_out = 0;
@@ -1625,6 +1652,21 @@ struct Batched {
     CK(cudaGetLastError());
     return SS_OK;
   }
+
+  // The stage launches of one step with every reduction, trajectory and arrest update
+  // off: reads the current fields, writes only workspace scratch (l1..l3, alternates).
+  static int timing_step(ss_batch* b) {
+    BatchStep B;
+    memset(&B, 0, sizeof(B));
+    B.wait_cycles = b->wait_cycles;
+    B.E_idx = -1;
+    B.err_idx = -1;
+    int rc = launch<M_S1>(b, B);
+    if (!rc) rc = b->tma ? launch<M_S23>(b, B) : launch<M_S2>(b, B);
+    if (!rc && !b->tma) rc = launch<M_S3>(b, B);
+    if (!rc) rc = launch<M_S4>(b, B);
+    return rc;
+  }
 };
 
 template <class Fn>
@@ -1636,6 +1678,48 @@ int batch_dispatch(const ss_batch* b, Fn&& fn) {
     case SS_THEORY_ANISOTROPIC: return fn((Anisotropic*)nullptr);
   }
   return fail(SS_ERR_ARG, "bad theory");
+}
+
+// tiles of a lattice in tile shape `shape`
+long long batch_tiles(const Grid& G, int shape) {
+  return (long long)((G.X + BSHAPE_TX[shape] - 1) / BSHAPE_TX[shape]) * ((G.Y + BSHAPE_TY[shape] - 1) / BSHAPE_TY[shape]);
+}
+
+// TMA maps of lattice i for its current tile shape (buffers already set); false when
+// a buffer or its row pitch is not 16-byte aligned
+bool batch_encode(ss_batch* b, int i) {
+  BatchInst& I = b->h_insts[i];
+  const int sh = b->shape[i];
+  bool ok = true;
+  for (int k = 0; k < 6 && ok; ++k)
+    ok = encode_tile_map(&I.tm[k], I.buf[k], b->elem, I.G.X, I.G.Y, b->nf, false, BSHAPE_TX[sh], BSHAPE_TY[sh]);
+  return ok;
+}
+
+// Rebuild the per-shape tile lists from the lattices with include[i] (all when null),
+// set each lattice's tile range and copy the descriptors and lists to the device.
+int batch_upload(ss_batch* b, const std::vector<char>* include) {
+  std::vector<int> lists[N_BATCH_SHAPES];
+  for (int i = 0; i < b->n; ++i) {
+    BatchInst& I = b->h_insts[i];
+    const int sh = b->shape[i];
+    I.ntiles = (int)batch_tiles(I.G, sh);
+    if (include && !(*include)[i]) {
+      I.tile0 = 0;
+      continue;
+    }
+    I.tile0 = (int)lists[sh].size();
+    lists[sh].insert(lists[sh].end(), (size_t)I.ntiles, i);
+  }
+  for (int g = 0; g < N_BATCH_SHAPES; ++g) {
+    b->group_tiles[g] = (int)lists[g].size();
+    if (!lists[g].empty())
+      CK(cudaMemcpyAsync(b->d_tile_inst[g], lists[g].data(), sizeof(int) * lists[g].size(), cudaMemcpyHostToDevice,
+                         b->stream));
+  }
+  CK(cudaMemcpyAsync(b->d_insts, b->h_insts.data(), sizeof(BatchInst) * b->n, cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return SS_OK;
 }
 
 }  // namespace
@@ -1664,15 +1748,17 @@ int ss_batch_create(int theory, int n_lattices, const int32_t* p_i, int n_i, con
       delete b;
       return fail(rc, "lattice %d: %s", i, msg);
     }
-    const long long t = (long long)((h.G.X + TX - 1) / TX) * ((h.G.Y + TY - 1) / TY);
-    b->tiles.push_back((int)t);
+    // partials and tile lists are sized for the finest shape the precision may use
+    const long long t = std::max(batch_tiles(h.G, 0), precision == SS_FP32 ? batch_tiles(h.G, 1) : 0LL);
+    b->max_tiles.push_back((int)std::min(t, 0x7fffffffLL));
     total += t;
   }
   if (total > 0x7fffffffLL) {
     delete b;
     return fail(SS_ERR_ARG, "batch too large");
   }
-  b->total_tiles = (int)total;
+  b->total_max = (int)total;
+  b->shape.assign(n_lattices, 0);
   b->nf = b->inst[0].nf;
   *out = b;
   return SS_OK;
@@ -1705,8 +1791,6 @@ int ss_batch_bind(ss_batch* b, void* const* fields, void* const* velocities, voi
   b->fields.assign(fields, fields + b->n);
   b->vels.assign(velocities, velocities + b->n);
   bool tma = true;
-  int tile0 = 0;
-  std::vector<int> tile_inst(b->total_tiles);
   for (int i = 0; i < b->n; ++i) {
     BatchInst& I = b->h_insts[i];
     if (!fields[i] || !velocities[i]) return fail(SS_ERR_ARG, "lattice %d: NULL field or velocity", i);
@@ -1714,23 +1798,16 @@ int ss_batch_bind(ss_batch* b, void* const* fields, void* const* velocities, voi
     I.P = b->inst[i].P;
     I.buf[0] = fields[i];
     I.buf[1] = velocities[i];
-    I.tile0 = tile0;
-    I.ntiles = b->tiles[i];
-    for (int t = 0; t < I.ntiles; ++t) tile_inst[tile0 + t] = i;
-    tile0 += I.ntiles;
-    for (int k = 0; k < 6 && tma; ++k) tma = encode_tile_map(&I.tm[k], I.buf[k], b->elem, I.G.X, I.G.Y, b->nf);
+    if (tma) tma = batch_encode(b, i);
   }
   b->tma = tma;
+  if (!tma) b->shape.assign(b->n, 0);  // the small shape is built for TMA staging only
   StepState init;
   memset(&init, 0, sizeof(init));
   init.E_last = NAN;
   const std::vector<StepState> inits(b->n, init);  // pageable: staged before the call returns
   CK(cudaMemcpyAsync(b->d_st, inits.data(), sizeof(StepState) * b->n, cudaMemcpyHostToDevice, b->stream));
-  CK(cudaMemcpyAsync(b->d_insts, b->h_insts.data(), sizeof(BatchInst) * b->n, cudaMemcpyHostToDevice, b->stream));
-  CK(cudaMemcpyAsync(b->d_tile_inst, tile_inst.data(), sizeof(int) * b->total_tiles, cudaMemcpyHostToDevice,
-                     b->stream));
-  CK(cudaStreamSynchronize(b->stream));
-  return SS_OK;
+  return batch_upload(b, nullptr);
 }
 
 int ss_batch_step(ss_batch* b, int n_steps, const double* prev_energy, double* energy_traj, double* err_traj) {
@@ -1782,6 +1859,94 @@ int ss_batch_step(ss_batch* b, int n_steps, const double* prev_energy, double* e
 }
 
 int ss_batch_tma_enabled(const ss_batch* b) { return b && b->tma ? 1 : 0; }
+
+int ss_batch_get_shape(const ss_batch* b, int lattice) {
+  if (!b || lattice < 0 || lattice >= b->n) return -1;
+  return b->shape[lattice];
+}
+
+int ss_batch_set_shape(ss_batch* b, int lattice, int shape) {
+  if (!b || !b->ws) return fail(SS_ERR_STATE, "batch not bound");
+  if (lattice < 0 || lattice >= b->n) return fail(SS_ERR_ARG, "lattice %d out of range", lattice);
+  if (shape < 0 || shape >= N_BATCH_SHAPES) return fail(SS_ERR_ARG, "tile shape %d: 0 (16 x 64) or 1 (8 x 32)", shape);
+  if (shape != 0 && (!b->tma || b->precision != SS_FP32))
+    return fail(SS_ERR_ARG, "the 8 x 32 tile shape needs TMA-staged FP32 lattices");
+  b->shape[lattice] = shape;
+  if (!batch_encode(b, lattice)) return fail(SS_ERR_CUDA, "tensor map of lattice %d", lattice);
+  return batch_upload(b, nullptr);
+}
+
+int ss_batch_autotune(ss_batch* b, int iters, float* ms_out) {
+  if (!b || !b->ws) return fail(SS_ERR_STATE, "batch not bound");
+  if (iters < 1) iters = 1;
+  if (ms_out)
+    for (int i = 0; i < 2 * b->n; ++i) ms_out[i] = 0.f;
+  if (!b->tma || b->precision != SS_FP32) return SS_OK;  // one tile shape only
+  // size classes: lattices of equal extents
+  std::vector<int> cls(b->n, -1);
+  std::vector<std::pair<int, int>> keys;
+  for (int i = 0; i < b->n; ++i) {
+    const std::pair<int, int> k(b->inst[i].G.X, b->inst[i].G.Y);
+    size_t c = 0;
+    while (c < keys.size() && keys[c] != k) ++c;
+    if (c == keys.size()) keys.push_back(k);
+    cls[i] = (int)c;
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  std::vector<float> ms(keys.size() * N_BATCH_SHAPES, 0.f);
+  int rc = SS_OK;
+  for (size_t c = 0; c < keys.size() && rc == SS_OK; ++c) {
+    std::vector<char> inc(b->n, 0);
+    for (int i = 0; i < b->n; ++i) inc[i] = cls[i] == (int)c;
+    for (int sh = 0; sh < N_BATCH_SHAPES && rc == SS_OK; ++sh) {
+      for (int i = 0; i < b->n; ++i)
+        if (inc[i]) {
+          b->shape[i] = sh;
+          batch_encode(b, i);
+        }
+      if ((rc = batch_upload(b, &inc))) break;
+      auto time_steps = [&](int n) -> int {
+        return batch_dispatch(b, [&](auto* tag) -> int {
+          using TH = std::remove_pointer_t<decltype(tag)>;
+          for (int k = 0; k < n; ++k) {
+            const int r = Batched<TH, float>::timing_step(b);
+            if (r) return r;
+          }
+          return SS_OK;
+        });
+      };
+      if ((rc = time_steps(1))) break;  // warm-up
+      if (cudaEventRecord(e0, b->stream) != cudaSuccess) { rc = fail(SS_ERR_CUDA, "cudaEventRecord"); break; }
+      if ((rc = time_steps(iters))) break;
+      if (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = fail(SS_ERR_CUDA, "timing the batch's tile shapes");
+        break;
+      }
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      ms[c * N_BATCH_SHAPES + sh] = t / iters;
+    }
+    const int best = ms[c * N_BATCH_SHAPES + 1] < ms[c * N_BATCH_SHAPES] ? 1 : 0;
+    for (int i = 0; i < b->n; ++i)
+      if (inc[i]) {
+        b->shape[i] = rc == SS_OK ? best : 0;
+        batch_encode(b, i);
+      }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const int up = batch_upload(b, nullptr);
+  if (rc) return rc;
+  if (up) return up;
+  if (ms_out)
+    for (int i = 0; i < b->n; ++i)
+      for (int sh = 0; sh < N_BATCH_SHAPES; ++sh) ms_out[2 * i + sh] = ms[cls[i] * N_BATCH_SHAPES + sh];
+  // the timing steps ran the stages with every state update off; only the ticket and
+  // err slots they reset were touched
+  return SS_OK;
+}
 
 }  // extern "C"
 

@@ -35,15 +35,16 @@ struct BatchStep {
 
 // Resident CTAs per SM the batched stage kernels are built for.  Each CTA stages,
 // computes and stores one tile, so the staging latency is hidden only by other
-// resident CTAs: FP32 fields cap the registers for three (85 per thread) instead of
-// the two that the heavier stencils (the Baby Skyrme term) would otherwise get.
-template <typename R, int MODE>
+// resident CTAs: FP32 fields cap the registers for three 256-thread CTAs (85 per
+// thread) instead of the two that the heavier stencils (the Baby Skyrme term) would
+// otherwise get, and for six 128-thread CTAs of the small 8 x 32 tiles.
+template <typename R, int MODE, int NT>
 __host__ __device__ constexpr int batch_ctas() {
-  return sizeof(R) == 4 ? 3 : 1;
+  return sizeof(R) == 4 ? (NT <= 128 ? 6 : 3) : 1;
 }
 
 template <class TH, typename R, int TX, int TY, int NT, bool TMA, int MODE>
-__global__ void __launch_bounds__(NT, (batch_ctas<R, MODE>()))
+__global__ void __launch_bounds__(NT, (batch_ctas<R, MODE, NT>()))
     batch_flow_kernel(const BatchInst* __restrict__ insts, const int* __restrict__ tile_inst,
                       const __grid_constant__ BatchStep B) {
   extern __shared__ __align__(128) unsigned char smem_raw[];

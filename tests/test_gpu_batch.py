@@ -240,3 +240,49 @@ def test_graph_replay_equals_stream_steps():
     for a, c in zip(res[0][0], res[1][0]):
         np.testing.assert_array_equal(a, c)
     np.testing.assert_array_equal(res[0][1], res[1][1])
+
+
+def test_batch_tile_shapes_autotune_and_agree():
+    """The autotuner times every size class in both tile shapes (16 x 64 and 8 x 32 sites)
+    and keeps one per class; whatever the shapes, every lattice's fields after five steps are
+    bitwise those of the 16 x 64 run (the per-site arithmetic does not depend on the tile),
+    and the energies agree to rounding (the per-tile partials are summed in another order)."""
+    th = load_theory("Baby Skyrme")
+    sizes = [(64, 64), (64, 64), (128, 96), (96, 128), (128, 96)]
+    rng = np.random.default_rng(9)
+    params = [th.params.default_params(xlen=X, ylen=Y, lsx=0.1, lsy=0.1, time_step=0.02,
+                                       kappa=float(rng.uniform(0.5, 2)), mpi=float(rng.uniform(0.5, 2)),
+                                       unit_magnetization=True) for X, Y in sizes]
+    fields = [_hedgehog(p.resolved(), B=i % 3 + 1, R=1.5, seed=i) for i, p in enumerate(params)]
+    runs = []
+    for mode in ("shape0", "shape1", "tuned"):
+        b = BatchSolver(th, params, "fp32")
+        assert b.tma_enabled
+        if mode == "shape1":
+            for i in range(len(sizes)):
+                b.set_shape(i, 1)
+            assert all(b.shape(i) == 1 for i in range(len(sizes)))
+        elif mode == "tuned":
+            tuned = b.autotune(2)
+            assert set(tuned) == {(64, 64), (128, 96), (96, 128)}
+            for ms0, ms1, chosen in tuned.values():
+                assert ms0 > 0 and ms1 > 0 and chosen == (1 if ms1 < ms0 else 0)
+        for i, F in enumerate(fields):
+            b.load(i, F)
+        E, _ = b.step(5, 1e300)
+        runs.append((E, [f.cpu().numpy() for f in b.fields]))
+    for E, fs in runs[1:]:
+        np.testing.assert_allclose(E, runs[0][0], rtol=1e-12)
+        for a, c in zip(fs, runs[0][1]):
+            np.testing.assert_array_equal(a, c)
+
+
+def test_batch_small_shape_rejected_without_tma():
+    th = load_theory("Baby Skyrme")
+    params = [th.params.default_params(xlen=33, ylen=70, lsx=0.1, lsy=0.1, unit_magnetization=True)]
+    b = BatchSolver(th, params, "fp32")
+    assert not b.tma_enabled
+    with pytest.raises(ValueError, match="TMA"):
+        b.set_shape(0, 1)
+    tuned = b.autotune(1)
+    assert list(tuned.values())[0][2] == 0
