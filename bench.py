@@ -40,6 +40,9 @@ UNIT = "Mpoint-updates/s"
 # words of nf components moved per site and step: S1 2, S2 3, S3 4, S4 7 as four
 # kernels; S1 2, S2+S3 fused 5, S4 7 when stages 2 and 3 run as one kernel
 WORDS_SEPARATE, WORDS_FUSED = 16, 14
+# end to end: one host->device load of the field and velocity, E2E_CALLS one-step
+# Simulation.step calls (each returns E and err to the host), one device->host read-back
+E2E_CALLS = 100
 
 
 def chiral_params(xlen=None, ylen=None, xsize=None):
@@ -285,7 +288,8 @@ def gpu_arm(args, rank, world, local_rank):
     host_F = F0.to(torch.float32).cpu().pin_memory()
     host_V = torch.zeros_like(host_F).pin_memory()
     out_F = torch.empty_like(host_F).pin_memory()
-    Ke = max(K // 2, 3)
+    # a fixed number of one-step calls, so the figure does not depend on the timed K
+    Ke = E2E_CALLS
     barrier()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -324,7 +328,9 @@ def gpu_arm(args, rank, world, local_rank):
                              "algorithmic_bytes_per_step": bytes_step},
                 "cpu_baseline": cpu, "cpu_baseline_port": cpu_port,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "steps": Ke, "api": "Simulation.step(prev_energy) per step"},
+                        "steps": Ke, "api": "Simulation.step(prev_energy) per step",
+                        "note": f"pinned host field+velocity in once, {Ke} one-step calls each returning (E, err), "
+                                "field out once; wall clock, max over ranks"},
                 "gpu_launches": launches, "clocks": clk.summary(),
                 "autotune": {**{f"S{m}": {"tile_per_cta_ms": a, "pipelined_ms": b, "chosen": "pipelined" if c else
                                           "tile_per_cta"} for m, (a, b, c) in tuning.items() if m != 6},
@@ -415,22 +421,33 @@ def relaxed_accuracy(dev, tol=1e-6, plain_steps=20_000):
     return out
 
 
-def c5_workflow(dev, tol=1e-5, max_steps=800_000, rel_delta=1e-2, fd_steps=400_000):
+def c5_workflow(dev, tol=1e-5, max_steps=300_000, rel_delta=1e-2, fd_steps=200_000, adjoint_steps=20_000,
+                log_path=None):
     """The large chiral magnet end to end: the workload's 4096^2 lattice (64 anti-skyrmions,
     B = 0.2 T, Heusler, demag on) relaxed by Simulation.minimize(tol) (FP32 arrested flow
     to its energy plateau, then FP64 on the projected state), its topological charge, and
-    dE_min/dB, dE_min/dD from the discretisation-consistent adjoint
-    (relaxed_coupling_gradients) against central differences of relaxed energies at
-    c (1 +- rel_delta), each relaxed by the same minimize from the relaxed state
-    (fd_steps steps at most).  The undamped RK4 dynamics is unstable for this saddle
-    system (see the module docstring), so the first 2000 steps are steps of the arrested
-    flow too.  Central-difference truncation at rel_delta = 1e-2: ~1e-5 relative."""
+    dE_min/dB, dE_min/dD from the envelope theorem (and the discretisation-corrected
+    relaxed_coupling_gradients) against central differences of relaxed energies at
+    c (1 +- rel_delta).  Each shifted lattice relaxes from the relaxed state by the FP32
+    flow to its energy plateau and contributes its FP64 projected energy: FP32 resolves
+    the energy to ~1e-9 relative, far below the 1e-4 the check needs (the difference is
+    ~1e-2 of E).  The undamped RK4 dynamics is unstable for this saddle system (see the
+    module docstring), so the first 2000 steps are steps of the arrested flow too.
+    Central-difference truncation at rel_delta = 1e-2: ~1e-5 relative.  With log_path,
+    the results so far are written there after every phase."""
     import torch
-    from soliton_solver_b200.autograd import coupling_gradients, relaxed_coupling_gradients
+    from soliton_solver_b200.autograd import relaxed_coupling_gradients
     from soliton_solver_b200.core.simulation import Simulation
     from soliton_solver_b200.initial_conditions import skyrmion_lattice
+
     th, p = chiral_params()
-    out = {"config": config({"tol": tol, "rel_delta": rel_delta})}
+    out = {"config": config({"tol": tol, "rel_delta": rel_delta, "max_steps": max_steps, "fd_steps": fd_steps})}
+
+    def log():
+        if log_path:
+            with open(log_path, "w") as fh:
+                json.dump(out, fh, default=float)
+
     sim = Simulation(p, th, precision="fp32", device=dev)
     sim.load_field(skyrmion_lattice(sim.rp, n=8, R=1.0, seed=1000, device=dev))
     out["Q0"] = sim.observables()["skyrmion_number"]
@@ -443,14 +460,16 @@ def c5_workflow(dev, tol=1e-5, max_steps=800_000, rel_delta=1e-2, fd_steps=400_0
     out["Q"] = obs["skyrmion_number"]
     out["Q_dev_from_integer"] = abs(obs["skyrmion_number"] - round(obs["skyrmion_number"]))
     out["energy"] = res["energy"]
+    log()
     t0 = time.perf_counter()
-    g_plain = coupling_gradients(sim, names=("B", "D"))  # envelope at the FP32 buffers (rounded)
-    g, info = relaxed_coupling_gradients(sim, names=("B", "D"))
+    g, info = relaxed_coupling_gradients(sim, names=("B", "D"), max_steps=adjoint_steps)
     out["adjoint_wall_s"] = time.perf_counter() - t0
     out["adjoint"] = g
-    out["adjoint_info"] = {k: v for k, v in info.items()}
-    out["envelope_fp32_state"] = g_plain
+    out["adjoint_info"] = dict(info)
+    log()
     F64 = sim.Field64.clone()
+    del sim
+    torch.cuda.empty_cache()
     fd = {}
     t0 = time.perf_counter()
     for name in ("B", "D"):
@@ -458,19 +477,19 @@ def c5_workflow(dev, tol=1e-5, max_steps=800_000, rel_delta=1e-2, fd_steps=400_0
         d = rel_delta * c
         Es = []
         for sgn in (1, -1):
-            ps = p.with_(**{name: c + sgn * d})
-            s2 = Simulation(ps, th, precision="fp32", device=dev)
+            s2 = Simulation(p.with_(**{name: c + sgn * d}), th, precision="fp32", device=dev)
             s2.load_field(F64)
-            r2 = s2.minimize(tol=tol, max_steps=fd_steps)
-            Es.append((r2["energy"], r2["steps"], r2["converged"]))
+            r2 = s2.minimize(tol=tol, max_steps=fd_steps, schedule="fp32")
+            Es.append((s2.projected_energy(), r2["steps"], r2["phases"][0]["stop"]))
             del s2
             torch.cuda.empty_cache()
-        fd[name] = {"fd": (Es[0][0] - Es[1][0]) / (2 * d), "steps": [Es[0][1], Es[1][1]], "delta": d,
-                    "converged": [Es[0][2], Es[1][2]]}
+        fd[name] = {"fd": (Es[0][0] - Es[1][0]) / (2 * d), "delta": d, "steps": [Es[0][1], Es[1][1]],
+                    "stop": [Es[0][2], Es[1][2]], "energies": [Es[0][0], Es[1][0]]}
         fd[name]["rel_err_adjoint"] = abs(g[name] - fd[name]["fd"]) / abs(fd[name]["fd"])
         fd[name]["rel_err_uncorrected"] = abs(info["uncorrected"][name] - fd[name]["fd"]) / abs(fd[name]["fd"])
-    out["fd_wall_s"] = time.perf_counter() - t0
-    out["finite_differences"] = fd
+        out["finite_differences"] = fd
+        out["fd_wall_s"] = time.perf_counter() - t0
+        log()
     return out
 
 
@@ -771,6 +790,12 @@ def main():
                                                        "initial_condition", "dat_field_dump", "fused_fp64",
                                                        "reference_numba_gpu"],
                     help="run only this block of the comparison and print it as one JSON line (profiling)")
+    ap.add_argument("--section", default="", choices=["", "accuracy", "batched_sweep", "graph_320", "render_rgba",
+                                                       "initial_condition", "dat_field_dump", "fused_fp64",
+                                                       "reference_numba_gpu"],
+                    help="run only this block of the comparison and print it as one JSON line (profiling)")
+    ap.add_argument("--workflow-log", default="", help="with --workflow: write the results so far to this file "
+                                                       "after every phase")
     ap.add_argument("--workflow", default="", choices=["", "c5"],
                     help="c5: relax the workload's lattice to tol and check dE/dB, dE/dD against finite "
                          "differences (minutes of GPU time; prints one JSON line)")
@@ -800,11 +825,26 @@ def main():
                   "fused_fp64": lambda d: fused_fp64(d, F0)}[args.section]
         print(json.dumps({"section": args.section, **fn(dev)}, default=float), flush=True)
         return 0
+    if args.section:
+        import torch
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        fn = {"accuracy": relaxed_accuracy, "batched_sweep": batched_sweep, "graph_320": small_lattice_graph,
+              "initial_condition": initial_condition, "reference_numba_gpu": lambda d: reference_numba_gpu()}.get(
+            args.section)
+        if fn is None:  # the blocks that work on the workload's field
+            from soliton_solver_b200.initial_conditions import skyrmion_lattice
+            th, p = chiral_params()
+            F0 = skyrmion_lattice(p.resolved(), n=8, R=1.0, seed=1000, device=dev)
+            fn = {"render_rgba": lambda d: render_rgba(d, F0), "dat_field_dump": lambda d: dat_field_dump(d, F0),
+                  "fused_fp64": lambda d: fused_fp64(d, F0)}[args.section]
+        print(json.dumps({"section": args.section, **fn(dev)}, default=float), flush=True)
+        return 0
     if args.workflow == "c5":
         import torch
         dev = torch.device("cuda", local_rank)
         torch.cuda.set_device(dev)
-        print(json.dumps(c5_workflow(dev), default=float), flush=True)
+        print(json.dumps(c5_workflow(dev, log_path=args.workflow_log or None), default=float), flush=True)
         return 0
     if world > 1:
         import datetime

@@ -61,15 +61,15 @@ def test_exact_gradient_is_the_derivative_of_the_energy_sum(name, key, kw):
         assert abs(an - fd) <= 1e-9 * max(abs(fd), 1e-3), (an, fd)
 
 
-def _smooth_skyrmion(rp):
-    """A skyrmion with the smooth profile f = pi exp(-r^2/2) (no cusp at its centre)."""
+def _smooth_skyrmion(rp, R=1.0):
+    """The Belavin-Polyakov skyrmion m = (2 R x, 2 R y, r^2 - R^2) / (r^2 + R^2): analytic
+    everywhere (profiles such as pi exp(-r/R) or pi exp(-r^2/2) leave non-analytic terms at
+    the centre, where the 4th-order stencils' error does not shrink like h^4)."""
     x = (torch.arange(rp.xlen, dtype=torch.float64) - (rp.xlen - 1) / 2)[:, None] * rp.lsx
     y = (torch.arange(rp.ylen, dtype=torch.float64) - (rp.ylen - 1) / 2)[None, :] * rp.lsy
-    r2 = x * x + y * y
-    f = torch.pi * torch.exp(-0.5 * r2)
-    th = torch.atan2(y.expand_as(r2), x.expand_as(r2))
-    m = torch.stack([torch.sin(f) * torch.cos(th), torch.sin(f) * torch.sin(th), torch.cos(f),
-                     torch.zeros_like(f)])
+    x, y = x.expand(rp.xlen, rp.ylen), y.expand(rp.xlen, rp.ylen)
+    d = x * x + y * y + R * R
+    m = torch.stack([2 * R * x / d, 2 * R * y / d, (x * x + y * y - R * R) / d, torch.zeros_like(d)])
     return m.reshape(-1).cuda()
 
 

@@ -7,7 +7,8 @@ demag on, B = 0.2 T, 64 anti-skyrmions on a jittered lattice, arrested Newton fl
     the rows within 4 stages x 2 cells, and the cut's masks reach 2 more): every site
     of the new field to 1e-5 absolute (the FP32 trajectory tolerance of the parity
     tests), the stage-4 err to 1e-4 x its scale, and the step's flow energy against
-    the oracle's FP64 energy of its new field to 1e-6 relative.
+    the oracle's FP64 energy of its new field: the projected FP64 energy of the stored result
+    to 1e-7, the flow's FP32-jet energy to 5e-6 (its stored-pole bias, 2.1e-6 here).
 
 Size-independent properties besides:
 
@@ -192,4 +193,8 @@ def test_fullsize_whole_lattice_step_vs_oracle(full):
     assert abs(float(err[0]) - err_want) <= 1e-4 * max(abs(err_want), 1.0)
     p_i, p_f = th.params.pack_device_params(rp)
     E_want = ref.energy("chiral_magnet", want, p_i, p_f)
-    assert abs(float(E[0]) - E_want) <= 1e-6 * abs(E_want)
+    # the FP64 energy of the stored FP32 result with its unit vectors renormalised in FP64
+    assert abs(sim.projected_energy() - E_want) <= 1e-7 * abs(E_want)
+    # the flow's own energy (FP32 jets) carries the stored-pole bias of the FP32 vacuum
+    # (m3 rounds to 1 where |m_perp| < 2.4e-4): 2.1e-6 relative on this lattice
+    assert abs(float(E[0]) - E_want) <= 5e-6 * abs(E_want)

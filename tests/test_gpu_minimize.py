@@ -50,7 +50,8 @@ def test_c2_default_schedule_meets_the_1e6_gate(c2_fp64_minimum):
     # the relaxed state lands in the Simulation's FP32 buffers and, in FP64, in sim.Field64
     assert sim.Field64.dtype == torch.float64
     assert abs(sim.observables()["skyrmion_number"] - round(sim.observables()["skyrmion_number"])) < 1e-4
-    assert len(res["trajectory"]["energy"]) == res["steps"]
+    # whole chunks are recorded; the run stops inside the last one, at the step below tol
+    assert 0 <= len(res["trajectory"]["energy"]) - res["steps"] < 1000
 
 
 def test_minimize_fp32_only_and_argument_checks():
