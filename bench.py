@@ -790,10 +790,6 @@ def main():
                                                        "initial_condition", "dat_field_dump", "fused_fp64",
                                                        "reference_numba_gpu"],
                     help="run only this block of the comparison and print it as one JSON line (profiling)")
-    ap.add_argument("--section", default="", choices=["", "accuracy", "batched_sweep", "graph_320", "render_rgba",
-                                                       "initial_condition", "dat_field_dump", "fused_fp64",
-                                                       "reference_numba_gpu"],
-                    help="run only this block of the comparison and print it as one JSON line (profiling)")
     ap.add_argument("--workflow-log", default="", help="with --workflow: write the results so far to this file "
                                                        "after every phase")
     ap.add_argument("--workflow", default="", choices=["", "c5"],
@@ -810,21 +806,6 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank, world)
-    if args.section:
-        import torch
-        dev = torch.device("cuda", local_rank)
-        torch.cuda.set_device(dev)
-        fn = {"accuracy": relaxed_accuracy, "batched_sweep": batched_sweep, "graph_320": small_lattice_graph,
-              "initial_condition": initial_condition, "reference_numba_gpu": lambda d: reference_numba_gpu()}.get(
-            args.section)
-        if fn is None:  # the blocks that work on the workload's field
-            from soliton_solver_b200.initial_conditions import skyrmion_lattice
-            th, p = chiral_params()
-            F0 = skyrmion_lattice(p.resolved(), n=8, R=1.0, seed=1000, device=dev)
-            fn = {"render_rgba": lambda d: render_rgba(d, F0), "dat_field_dump": lambda d: dat_field_dump(d, F0),
-                  "fused_fp64": lambda d: fused_fp64(d, F0)}[args.section]
-        print(json.dumps({"section": args.section, **fn(dev)}, default=float), flush=True)
-        return 0
     if args.section:
         import torch
         dev = torch.device("cuda", local_rank)
