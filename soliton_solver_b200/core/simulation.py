@@ -173,7 +173,7 @@ class Simulation:
         if schedule != "fp64" and self.precision != "fp32":
             raise ValueError(f"schedule {schedule!r} needs an FP32 Simulation")
         N = self.rp.dim_grid
-        chunk = int(chunk) if chunk else (1000 if N <= (1 << 20) else 200)
+        chunk = int(chunk) if chunk else 1000
         out = {"schedule": schedule, "tol": tol, "phases": [], "steps": 0}
         traj = {"energy": [], "err": [], "precision": [], "projected": []}
         budget = int(max_steps)

@@ -6,9 +6,12 @@
    is exact for energies of degree <= 4 in the field (all four theories) up to rounding;
    tolerance 1e-9 relative.  The residual X - S (S: the flow's stencil derivative) shrinks
    like h^4 under refinement in the interior.
-2. relaxed_coupling_gradients on the chiral magnet at h = 10/255 (where the envelope value at
-   the flow's relaxed state is off by ~4e-4): the corrected dE_min/dB matches central
+2. relaxed_coupling_gradients on the chiral magnet at h = 10/255, where the envelope value at
+   the flow's relaxed state is off by ~4.6e-4 (the flow's stencil gradient is not the
+   derivative of the discrete energy: O(h^4) inside, O(1/h) next to the frozen ring): with
+   the adjoint's linear-response correction (one MINRES solve) dE_min/dB matches central
    differences of relaxed energies to 1e-5.
+3. ss_set_forcing adds a fixed field to the flow's gradient in every stage.
 """
 import numpy as np
 import pytest
@@ -111,5 +114,51 @@ def test_corrected_chiral_adjoint_matches_finite_differences():
     _, Ep = _relaxed(th, dict(kw, B=kw["B"] + d), lambda rp: F, 40000)
     _, Em = _relaxed(th, dict(kw, B=kw["B"] - d), lambda rp: F, 40000)
     fd = (Ep - Em) / (2 * d)
-    assert abs(plain - fd) > 1e-4 * abs(fd)  # the O(h^4) gap this spacing shows uncorrected
+    assert abs(plain - fd) > 1e-4 * abs(fd)  # the discretisation gap this spacing shows uncorrected
     assert abs(g["B"] - fd) <= 1e-5 * abs(fd), (g["B"], plain, fd, info)
+    assert info["minres_iterations"] < 20000
+
+
+def test_forcing_is_added_to_the_flow_gradient():
+    """ss_set_forcing: FP64 flow steps with a fixed field f added to the gradient rows equal
+    the oracle's arrested-Newton steps with EG + f in every RK4 stage (Abelian Higgs: no
+    projection, no halo zeroing, no row scaling), to 1e-12; removing it restores the flow."""
+    th = load_theory("Abelian Higgs")
+    rp = th.params.default_params(xlen=24, ylen=20, xsize=2.3, ysize=1.9, Lambda=0.7).resolved()
+    p_i, p_f = th.params.pack_device_params(rp)
+    rng = np.random.default_rng(8)
+    F = 0.3 * rng.standard_normal((4, 24, 20))
+    F[2] += 0.8
+    f = 0.1 * rng.standard_normal(F.shape)
+    dt = float(p_f[5])
+
+    def forced_step(F, V, prev):
+        def l(T):
+            return -dt * (ref.gradient_step("ginzburg_landau_superconductor", T, p_i, p_f)[1] + f)
+        k1, T = ref.rk4_stage(V, V, F, F, 0.0, p_f)
+        l1 = l(T)
+        k2, T = ref.rk4_stage(V, l1, F, k1, 0.5, p_f)
+        l2 = l(T)
+        k3, T = ref.rk4_stage(V, l2, F, k2, 0.5, p_f)
+        l3 = l(T)
+        k4, T = ref.rk4_stage(V, l3, F, k3, 1.0, p_f)
+        l4 = l(T)
+        Vn, Fn = ref.rk4_finalize("ginzburg_landau_superconductor", V, F, k1, k2, k3, k4, l1, l2, l3, l4, p_i)
+        E = ref.energy("ginzburg_landau_superconductor", Fn, p_i, p_f)
+        return Fn, (np.zeros_like(Vn) if E > prev else Vn), E
+
+    s = Solver(th.kernels.THEORY_ID, p_i, p_f, "fp64")
+    fd = torch.tensor(F.reshape(-1), device="cuda")
+    vd = torch.zeros_like(fd)
+    s.bind(fd, vd)
+    s.set_forcing(torch.tensor(f.reshape(-1), device="cuda"))
+    E, _ = s.step(2, 1e300)
+    Fo, Vo, prev = F, np.zeros_like(F), 1e300
+    for k in range(2):
+        Fo, Vo, prev = forced_step(Fo, Vo, prev)
+        assert abs(E[k] - prev) <= 1e-12 * abs(prev)
+    np.testing.assert_allclose(fd.cpu().numpy(), Fo.reshape(-1), rtol=0, atol=1e-12)
+    s.set_forcing(None)
+    E2, _ = s.step(1, float("nan"))
+    Fu, _, Eu, _ = ref.relax("ginzburg_landau_superconductor", Fo, Vo, prev, p_i, p_f, 1)
+    assert abs(E2[0] - Eu[0]) <= 1e-12 * abs(Eu[0])
