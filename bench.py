@@ -516,6 +516,7 @@ def batched_sweep(dev, steps=20, seed=4, reps=3):
     kappa, mpi ~ U(0.5, 2), windings B in 1..4, hedgehogs with R ~ U(1, 3), FP32 fields.
     Lattice spacing 0.1 and dt = 0.002: a winding-4 hedgehog with R = 1 and kappa = 2 has
     |grad m| ~ 13, so the Skyrme term's stiffness bounds the explicit step near h/26.
+    The autotuner first picks each size class's tile shape (ss_batch_autotune).  Then
     `steps` steps of every lattice are captured as one CUDA graph (ss_batch_graph_create:
     per step one launch per RK stage over all lattices' tiles, per-lattice energies and
     arrest on the device) and replayed `reps` times between CUDA events; the same steps
@@ -535,6 +536,7 @@ def batched_sweep(dev, steps=20, seed=4, reps=3):
     for i, p in enumerate(params):
         b.load(i, hedgehog(p.resolved(), charge=int(rng.integers(1, 5)), R=float(rng.uniform(1, 3)), seed=i,
                            device=dev))
+    tuned = b.autotune(3)  # tile shape per size class (16 x 64 or 8 x 32 sites)
     b.step(3, 1e300)
     sites = int(sum(int(e) * int(e) for e in edges))
     torch.cuda.synchronize(dev)
@@ -562,6 +564,8 @@ def batched_sweep(dev, steps=20, seed=4, reps=3):
             "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak, "bytes_per_point_update": 168,
             "stream_value": sites * steps / dt_stream / 1e6, "stream_ms_per_step": dt_stream / steps * 1e3,
             "tma": b.tma_enabled, "finite": bool(np.isfinite(E).all() and np.isfinite(Eg).all()),
+            "tile_shapes": {f"{k[0]}x{k[1]}": {"ms_16x64": v[0], "ms_8x32": v[1], "chosen": "8x32" if v[2] else "16x64"}
+                            for k, v in tuned.items()},
             "note": "one CUDA-graph launch per `steps` steps of all 256 lattices, CUDA events around the replays; "
                     "stream_value: ss_batch_step incl. its host synchronisation"}
 

@@ -171,18 +171,21 @@ def coupling_gradients(sim, names=None) -> dict:
     return _partials(sim, sim.solver, sim.Field, names)
 
 
-def _minres(apply, b, tol, max_iter, monitor=None, every=200):
-    """MINRES (Paige and Saunders) for the symmetric, possibly indefinite A x = b, from x = 0;
-    returns (x, iterations, relative residual).  monitor(x, it) is called every `every`
-    iterations and ends the solve when it returns True."""
+def _minres(apply, b, tol, max_iter, monitor=None, every=200, precond=None):
+    """Preconditioned MINRES (Paige and Saunders) for the symmetric, possibly indefinite
+    A x = b from x = 0, with the symmetric positive definite preconditioner precond(v) =
+    M^-1 v (identity when None); returns (x, iterations, relative preconditioned residual).
+    monitor(x, it) is called every `every` iterations and ends the solve when it returns
+    True."""
     import torch
+    minv = precond if precond is not None else (lambda v: v)
     x = torch.zeros_like(b)
-    beta1 = float(torch.linalg.vector_norm(b))
+    r1 = b.clone()
+    y = minv(r1)
+    beta1 = float(torch.dot(r1, y)) ** 0.5 if float(torch.dot(r1, y)) > 0 else 0.0
     if beta1 == 0.0:
         return x, 0, 0.0
-    r1 = b.clone()
-    r2 = b.clone()
-    y = b.clone()
+    r2 = r1.clone()
     w = torch.zeros_like(b)
     w2 = torch.zeros_like(b)
     oldb, beta, dbar, epsln, phibar, cs, sn = 0.0, beta1, 0.0, 0.0, beta1, -1.0, 0.0
@@ -195,7 +198,9 @@ def _minres(apply, b, tol, max_iter, monitor=None, every=200):
         alfa = float(torch.dot(v, y))
         y = y - (alfa / beta) * r2
         r1, r2 = r2, y
-        oldb, beta = beta, float(torch.linalg.vector_norm(y))
+        y = minv(r2)
+        oldb = beta
+        beta = max(float(torch.dot(r2, y)), 0.0) ** 0.5
         oldeps = epsln
         delta = cs * dbar + sn * alfa
         gbar = sn * dbar - cs * alfa
@@ -216,7 +221,7 @@ def _minres(apply, b, tol, max_iter, monitor=None, every=200):
 
 
 def relaxed_coupling_gradients(sim, names=None, tol: float = 1e-8, max_iter: int = 20000, eps: float = 1e-6,
-                               rtol: float = 1e-4):
+                               rtol: float = 1e-4, precondition: bool = True, shift: float = 1.0):
     """dE_min/dc at a relaxed field, with the discretisation correction of the adjoint.
 
     The flow relaxes to the zero of the reference's stencil gradient S (the 4th-order
@@ -233,8 +238,13 @@ def relaxed_coupling_gradients(sim, names=None, tol: float = 1e-8, max_iter: int
     along w (ss_energy_gradient, 2 evaluations per iteration, step eps relative to the
     largest entry of w), dS/dc by central differences in the coupling (solvers at
     c (1 +- 1e-4); S is linear in the reduced couplings but for the demag row's 1/coup_mu).
-    The solve stops at relative residual `tol`, after `max_iter` iterations, or when every
-    correction has moved by less than `rtol` of itself over the last 1000 iterations.
+    With `precondition`, MINRES runs with the symmetric positive definite preconditioner
+    P (shift - Laplacian)^-1 P (per component by FFT, periodic, second-order symbol; the
+    demag row scaled by coup_mu, whose true-row block is Laplacian / coup_mu with the
+    opposite sign): the spectrum of the preconditioned operator no longer spreads with
+    1/h^2 and the saddle's indefinite block costs no more than the rest.  The solve stops
+    at relative residual `tol`, after `max_iter` iterations, or when every correction has
+    moved by less than `rtol` of itself over the last 1000 iterations.
     The field is the FP64 relaxed state (sim.Field64 after a mixed-precision minimize,
     else sim.Field).  Returns (grads, info) with info = the envelope values, the
     corrections, MINRES iterations and relative residual.  The Simulation is not
@@ -283,6 +293,21 @@ def relaxed_coupling_gradients(sim, names=None, tol: float = 1e-8, max_iter: int
         step = eps / max(float(v.abs().max()), 1e-300)
         return project((flow_residual(F + step * v) - flow_residual(F - step * v)) / (2 * step))
 
+    precond = None
+    if precondition:
+        fx = torch.fft.fftfreq(X, device=F.device, dtype=torch.float64)[:, None]
+        fy = torch.fft.rfftfreq(Y, device=F.device, dtype=torch.float64)[None, :]
+        symbol = (4.0 / rp.lsx ** 2) * torch.sin(torch.pi * fx) ** 2 + (4.0 / rp.lsy ** 2) * torch.sin(torch.pi * fy) ** 2
+        inv_symbol = 1.0 / (symbol + shift)
+        scale = torch.ones(nf, 1, 1, dtype=torch.float64, device=F.device)
+        if sim.kernels.THEORY_ID == 0 and int(sim.p_i_h[15]):
+            scale[3] = float(sim.p_f_h[8])  # demag row: (shift - Laplacian) / coup_mu
+
+        def precond(v):
+            v = project(v).view(nf, X, Y)
+            z = torch.fft.irfft2(torch.fft.rfft2(v) * inv_symbol, s=(X, Y)) * scale
+            return project(z)
+
     r = s64.energy_gradient_exact(F, minus_stencil=True)
     b = project(r)
     g0 = _partials(sim, s64, F, names)
@@ -313,7 +338,7 @@ def relaxed_coupling_gradients(sim, names=None, tol: float = 1e-8, max_iter: int
         old = history[-6][1]  # the corrections 1000 iterations ago
         return all(abs(corr[k] - old[k]) <= rtol * max(abs(corr[k]), 1e-300) for k in corr)
 
-    w, iters, rel = _minres(apply, b, tol, max_iter, monitor if dS else None)
+    w, iters, rel = _minres(apply, b, tol, max_iter, monitor if dS else None, precond=precond)
     corr = {k: -dA * float(torch.dot(w, v)) for k, v in dS.items()}
     out = {k: g0[k] + corr.get(k, 0.0) for k in g0}
     info = {"uncorrected": g0, "correction": corr, "minres_iterations": iters, "minres_rel_residual": rel,
