@@ -399,7 +399,7 @@ def relaxed_accuracy(dev, tol=1e-6, plain_steps=20_000):
         else None
     mixed["projected_rel_at_switch"] = float(relp[-1]) if len(relp) else None
     mixed["rel_diff_vs_fp64"] = abs(mixed["energy"] - E_star) / abs(E_star)
-    # plain FP64 (the reference's structure on the GPU): bitwise the fused FP64 trajectory
+    # plain FP64 (the reference's structure on the GPU): the fused FP64 trajectory up to rounding
     p20 = Simulation(p, th, precision="plain_fp64", device=dev)
     f20 = Simulation(p, th, precision="fp64", device=dev)
     for sim in (p20, f20):
