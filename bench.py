@@ -37,9 +37,10 @@ XLEN = YLEN = 4096
 XSIZE = 128.0
 METRIC = "Mpoint-updates/s per flow step at dE/E<=1e-6 vs plain FP64; achieved HBM GB/s"
 UNIT = "Mpoint-updates/s"
-# words of nf components moved per site and step: S1 2, S2 3, S3 4, S4 7 as four
-# kernels; S1 2, S2+S3 fused 5, S4 7 when stages 2 and 3 run as one kernel
-WORDS_SEPARATE, WORDS_FUSED = 16, 14
+# words of nf components moved per site and step: S1 2 (phi in, l1 out), S2 3, S3 7
+# (phi, V, l1, l2 in; T4, cV, cP out), S4 5 (T4, cP, cV in; phi', V' out) as four
+# kernels; S1 2, S2+S3 fused 6, S4 5 when stages 2 and 3 run as one kernel
+WORDS_SEPARATE, WORDS_FUSED = 17, 13
 # end to end: one host->device load of the field and velocity, E2E_CALLS one-step
 # Simulation.step calls (each returns E and err to the host), one device->host read-back
 E2E_CALLS = 100
@@ -261,9 +262,10 @@ def gpu_arm(args, rank, world, local_rank):
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     ms_step = ms / K
     value = world * N * K / (ms / 1e3) / 1e6
-    launches = (3 if (s.tma_enabled and s._lib.ss_get_variant(s._h, 6) == 1) else 4) * K + 2
+    # stage launches per step, and the call's closing arrest kernel
+    launches = (3 if (s.tma_enabled and s._lib.ss_get_variant(s._h, 6) == 1) else 4) * K + 1
 
-    # roofline of the fused stage kernel (4 launches per step)
+    # roofline of the stage kernels (3 launches per step with stages 2 and 3 fused, else 4)
     from soliton_solver_b200._native import load as _load  # noqa: F401 (library loaded)
     peaks = {}
     try:
@@ -521,7 +523,7 @@ def batched_sweep(dev, steps=20, seed=4, reps=3):
     per step one launch per RK stage over all lattices' tiles, per-lattice energies and
     arrest on the device) and replayed `reps` times between CUDA events; the same steps
     issued by ss_batch_step (stream launches plus its per-call host copies) are timed
-    beside it.  Roofline: 14 words x 3 components x 4 bytes per point-update."""
+    beside it.  Roofline: 13 words x 3 components x 4 bytes per point-update."""
     import torch
     from soliton_solver_b200.core.batch import BatchSolver
     from soliton_solver_b200.initial_conditions import hedgehog
@@ -558,10 +560,10 @@ def batched_sweep(dev, steps=20, seed=4, reps=3):
     Eg, _ = b.trajectory()
     peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0)) \
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
-    gbs = sites * 14 * 3 * 4 / (ms / 1e3) / 1e9
+    gbs = sites * WORDS_FUSED * 3 * 4 / (ms / 1e3) / 1e9
     return {"lattices": 256, "sites": sites, "steps_per_graph": steps, "replays": reps,
             "value": sites / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms,
-            "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak, "bytes_per_point_update": 168,
+            "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak, "bytes_per_point_update": WORDS_FUSED * 3 * 4,
             "stream_value": sites * steps / dt_stream / 1e6, "stream_ms_per_step": dt_stream / steps * 1e3,
             "tma": b.tma_enabled, "finite": bool(np.isfinite(E).all() and np.isfinite(Eg).all()),
             "tile_shapes": {f"{k[0]}x{k[1]}": {"ms_16x64": v[0], "ms_8x32": v[1], "chosen": "8x32" if v[2] else "16x64"}

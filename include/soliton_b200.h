@@ -105,8 +105,9 @@ const char *ss_last_error(void);
 int ss_create(int theory, const int32_t *p_i, int n_i, const double *p_f, int n_f, int precision,
               ss_handle **out);
 int ss_destroy(ss_handle *h);
-/* Bytes of caller-owned device workspace ss_bind() needs (l1..l3, the Field/Velocity
- * ping-pong copies, reduction partials and the device-side step state). */
+/* Bytes of caller-owned device workspace ss_bind() needs (five field-sized flow
+ * buffers: l1, l2, the stage-4 field T4 and stage 4's two accumulated inputs; reduction
+ * partials and the device-side step state). */
 int ss_workspace_bytes(const ss_handle *h, size_t *bytes);
 /* Bind the caller's Field and Velocity buffers, the workspace and the stream. */
 int ss_bind(ss_handle *h, void *field, void *velocity, void *workspace, size_t workspace_bytes,
@@ -349,7 +350,7 @@ int ss_batch_set_shape(ss_batch *b, int lattice, int shape);
 
 /* ---- CUDA graphs ---------------------------------------------------------------
  * ss_graph_create captures n_steps of ss_step_async(h, n_steps, NaN, ...) — every
- * stage launch, the trailing energy pass and the copy-back — into a CUDA graph on a
+ * stage launch and the closing arrest kernel — into a CUDA graph on a
  * private stream; ss_graph_launch replays it on the bound stream (each replay
  * continues from the device state).  The batch versions capture n_steps (at most
  * 1024) of every lattice; ss_batch_trajectory copies the last replay's per-lattice

@@ -763,3 +763,21 @@ def relax(theory, F, V, prev_energy, p_i, p_f, n_steps):
         E_traj[s] = E
         err_traj[s] = err
     return F, V, E_traj, err_traj
+
+
+def relax_replay(theory, F, V, arrests, p_i, p_f):
+    """``len(arrests)`` flow steps of do_arrested_newton_flow (core/integrator.py:217-348)
+    with the arrest decisions given instead of taken: V = 0 after step s iff arrests[s].
+    An FP32 flow decides E' > E on FP32 energies, which cannot resolve the energy steps
+    near an arrest (|dE|/E ~ 1e-9 in a few hundred steps); replaying its decisions lets
+    its trajectory be compared step for step.  Returns (F, V, E_traj, err_traj)."""
+    n_steps = len(arrests)
+    E_traj = np.empty(n_steps)
+    err_traj = np.empty(n_steps)
+    for s in range(n_steps):
+        F, V, E, err = arrested_newton_flow_step(theory, F, V, np.inf, p_i, p_f)
+        if arrests[s]:
+            V = np.zeros_like(V)
+        E_traj[s] = E
+        err_traj[s] = err
+    return F, V, E_traj, err_traj

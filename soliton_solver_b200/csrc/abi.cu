@@ -30,6 +30,9 @@ namespace {
 constexpr int TX = 16, TY = 64, NT = 256;  // fused tile: 16 x 64 sites, 256 threads
 constexpr int TRAJ_CAP = 1024;              // device trajectory slots used by ss_step
 constexpr size_t ALIGN = 256;
+// TMA maps of a bound handle: halo boxes of the field, the velocity, l1 and T4 (l[2]),
+// and centre boxes of cP and cV
+enum { TM_FIELD = 0, TM_VEL = 1, TM_L1 = 2, TM_T4 = 3, TM_CP = 4, TM_CV = 5, TM_COUNT = 6 };
 
 thread_local char g_err[512] = "";
 
@@ -103,9 +106,11 @@ struct ss_handle {
   double* partial = nullptr;
   double* traj_E = nullptr;
   double* traj_err = nullptr;
+  // fused flow buffers: l1, l2 (four-kernel steps only), T4; then cP and cV (stage 4's
+  // inputs besides T4: phi + dt V + dt (l1 + l2 + l3)/6 and V + (l1 + 2 l2 + 2 l3)/6)
   void* l[4] = {nullptr, nullptr, nullptr, nullptr};
-  void* phi_alt = nullptr;
-  void* vel_alt = nullptr;
+  void* cp_buf = nullptr;
+  void* cv_buf = nullptr;
   // plain extras
   void* k[4] = {nullptr, nullptr, nullptr, nullptr};
   void* temp = nullptr;
@@ -116,9 +121,8 @@ struct ss_handle {
   double* entmp = nullptr;
   double E_last_host = NAN;
   std::vector<double> host_partial;
-  // TMA maps of the bound buffers: field, velocity, phi_alt, vel_alt, l1, l2 (halo
-  // boxes), then l1 and l3 centre boxes
-  CUtensorMap tm[8];
+  // TMA maps of the bound buffers (index constants TM_*)
+  CUtensorMap tm[TM_COUNT];
   bool tma = false;
   int num_sms = 148;
   // per flow mode: 1 = persistent pipelined kernel, 0 = one tile per CTA (autotuned)
@@ -168,8 +172,8 @@ size_t layout(ss_handle* h, char* base) {
   } else {
     for (int i = 0; i < 3; ++i) h->l[i] = take(field_bytes);
     h->l[3] = nullptr;
-    h->phi_alt = take(field_bytes);
-    h->vel_alt = take(field_bytes);
+    h->cp_buf = take(field_bytes);
+    h->cv_buf = take(field_bytes);
   }
   return off;
 }
@@ -331,7 +335,8 @@ struct Fused {
   }
 
   // threads of a one-tile CTA: 512 where the staged buffers leave room for only one CTA
-  // per SM (FP64 stages 3, 4 and 2+3, the six-component s+id in FP64), else 256
+  // per SM (above 113 KB: FP64 stages 3 and 2+3, and stage 2 of the six-component s+id
+  // in FP64), else 256
   template <bool TMA_, int MODE>
   static constexpr int flow_threads() {
     return flow_smem<TMA_, MODE>() > 113 * 1024 ? 2 * NT : NT;
@@ -447,173 +452,149 @@ struct Fused {
     return A;
   }
 
-  // n flow steps of the bound buffers; trajectories to device arrays (nullable)
+  // n flow steps of the bound buffers, in place; trajectories to device arrays (nullable)
   static int step(ss_handle* h, int n, double prev, double* E_dev, double* err_dev) {
     if (n <= 0) return SS_OK;
     R* field = (R*)h->field;
     R* vel = (R*)h->vel;
-    R* cur_p = field;
-    R* cur_v = vel;
-    R* alt_p = (R*)h->phi_alt;
-    R* alt_v = (R*)h->vel_alt;
     R* l1 = (R*)h->l[0];
     R* l2 = (R*)h->l[1];
-    R* l3 = (R*)h->l[2];
+    R* t4 = (R*)h->l[2];
+    R* cp = (R*)h->cp_buf;
+    R* cv = (R*)h->cv_buf;
     FlowArgs<R> A = base_args(h);
     A.E_traj = E_dev;
     A.err_traj = err_dev;
     const bool tma = h->tma;
-    // maps: [0] field [1] velocity [2] phi_alt [3] vel_alt [4] l1 [5] l2
-    int cur = 0;
+    const bool fused23 = tma && h->fuse23;
+    A.vel = vel;
+    A.la = l1;
+    A.lb = l2;
+    A.out_t4 = t4;
+    A.out_cp = cp;
+    A.out_cv = cv;
+    A.cp = cp;
+    A.cv = cv;
+    A.phi_out = field;
+    A.vel_out = vel;
+    if (tma) {
+      A.tm_vel = h->tm[TM_VEL];
+      A.tm_l = h->tm[TM_L1];
+      A.tm_cp = h->tm[TM_CP];
+      A.tm_cv = h->tm[TM_CV];
+    }
     for (int s = 0; s < n; ++s) {
-      // The last step of a call with an odd count reads the caller's buffers and would
-      // leave its result in the alternates (a copy back after the call).  Instead stage 2
-      // copies phi and V into the alternates on its way (it stages both anyway) and stage
-      // 4 reads them there and writes the result into the caller's buffers.
-      const bool land = s == n - 1 && cur == 0;
-      A.phi = cur_p;
-      A.vel = cur_v;
-      if (tma) {
-        A.tm_phi = h->tm[cur == 0 ? 0 : 2];
-        A.tm_vel = h->tm[cur == 0 ? 1 : 3];
-      }
       // S1: l1 = -dt G(phi); energy of phi (the previous step's result) + arrest test
       A.mode = M_S1;
+      A.phi = field;
       A.out_l = l1;
       A.with_energy = s > 0;
       A.arrest_update = s > 0;
       A.E_idx = s - 1;
       A.init_state = s == 0;
       A.prev_energy = prev;
+      if (tma) A.tm_phi = h->tm[TM_FIELD];
       int rc = launch(h, A, tma);
       if (rc) return rc;
       A.with_energy = 0;
       A.arrest_update = 0;
       A.init_state = 0;
       A.E_idx = -1;
-      // S2, S3: one fused kernel on TMA-staged buffers (one staging of phi, V, l1),
-      // else two
-      const bool fused23 = tma && h->fuse23;
-      const bool copy_in_s2 = land && (fused23 || !tma || !h->use_pipe[M_S2]);  // one tile per CTA
-      if (copy_in_s2) {
-        A.copy_phi = alt_p;
-        A.copy_vel = alt_v;
-      }
+      // S2, S3 (one fused kernel on TMA-staged buffers: one staging of phi, V, l1):
+      // T4, cV, cP
       if (fused23) {
         A.mode = M_S23;
-        A.la = l1;
-        A.out_l = l3;
-        A.out_l2 = l2;
-        A.tm_l = h->tm[4];
         if ((rc = launch(h, A, tma))) return rc;
-        A.out_l2 = nullptr;
       } else {
         A.mode = M_S2;
         A.out_l = l2;
         if ((rc = launch(h, A, tma))) return rc;
-        A.copy_phi = nullptr;
-        A.copy_vel = nullptr;
         A.mode = M_S3;
-        A.la = l1;
-        A.out_l = l3;
-        if (tma) A.tm_l = h->tm[4];
         if ((rc = launch(h, A, tma))) return rc;
       }
-      A.copy_phi = nullptr;
-      A.copy_vel = nullptr;
-      const size_t bytes = (size_t)h->nf * h->G.N * sizeof(R);
-      if (land && !copy_in_s2) {  // pipelined stage 2: plain copies
-        CK(cudaMemcpyAsync(alt_p, cur_p, bytes, cudaMemcpyDeviceToDevice, h->stream));
-        CK(cudaMemcpyAsync(alt_v, cur_v, bytes, cudaMemcpyDeviceToDevice, h->stream));
-      }
-      if (land) {  // stage 4 reads phi and V from the alternates, writes the caller's buffers
-        A.phi = alt_p;
-        A.vel = alt_v;
-        if (tma) {
-          A.tm_phi = h->tm[2];
-          A.tm_vel = h->tm[3];
-        }
-      }
-      // S4 + finalize into the ping-pong buffers
-      A.mode = M_S4;
-      A.la = l1;
-      A.lb = l2;
-      A.lc = l3;
       A.out_l = nullptr;
-      A.phi_out = land ? cur_p : alt_p;
-      A.vel_out = land ? cur_v : alt_v;
+      // S4: phi' and V' into the caller's buffers, err
+      A.mode = M_S4;
+      A.phi = t4;
       A.err_idx = s;
-      if (tma) {
-        A.tm_l = h->tm[5];
-        A.tm_c1 = h->tm[6];
-        A.tm_c3 = h->tm[7];
-      }
+      if (tma) A.tm_phi = h->tm[TM_T4];
       if ((rc = launch(h, A, tma))) return rc;
       A.err_idx = -1;
-      if (!land) {
-        std::swap(cur_p, alt_p);
-        std::swap(cur_v, alt_v);
-        cur ^= 1;
-      }
     }
     // trailing energy of the final field + arrest test
-    A.phi = cur_p;
+    A.phi = field;
     A.mode = M_ENERGY;
     A.with_energy = 1;
     A.arrest_update = 1;
     A.E_idx = n - 1;
-    if (tma) A.tm_phi = h->tm[cur == 0 ? 0 : 2];
+    if (tma) A.tm_phi = h->tm[TM_FIELD];
     int rc = launch(h, A, tma);
     if (rc) return rc;
     const long long nfN = (long long)h->nf * h->G.N;
-    finish_kernel<R><<<grid_1d(nfN), 256, 0, h->stream>>>(cur_p, cur_v, field, vel, nfN, cur_p != field ? 1 : 0,
-                                                          h->st);
+    finish_kernel<R><<<grid_1d(nfN), 256, 0, h->stream>>>(vel, nfN, h->st);
     CK(cudaGetLastError());
     return SS_OK;
   }
 
-  // Time both staging variants of every stage on the bound buffers (writes only
-  // workspace scratch: l1..l3 and the ping-pong copies) and keep the faster one.
+  // Time both staging variants of every stage on the bound buffers and keep the faster
+  // one.  Writes only workspace scratch: l1, l2, T4, cV, cP, and stage 4's phi' and V'
+  // into the l1 and l2 buffers (stage 4 reads neither); stage 1's energy reduction
+  // leaves the arrest state and the trajectories alone.
   static int autotune(ss_handle* h, int iters) {
     if (!h->tma) return SS_OK;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     FlowArgs<R> A = base_args(h);
-    A.phi = (const R*)h->field;
     A.vel = (const R*)h->vel;
     A.la = (const R*)h->l[0];
     A.lb = (const R*)h->l[1];
-    A.lc = (const R*)h->l[2];
-    A.phi_out = (R*)h->phi_alt;
-    A.vel_out = (R*)h->vel_alt;
-    A.tm_phi = h->tm[0];
-    A.tm_vel = h->tm[1];
-    A.tm_c1 = h->tm[6];
-    A.tm_c3 = h->tm[7];
+    A.out_t4 = (R*)h->l[2];
+    A.out_cp = (R*)h->cp_buf;
+    A.out_cv = (R*)h->cv_buf;
+    A.cp = (const R*)h->cp_buf;
+    A.cv = (const R*)h->cv_buf;
+    A.phi_out = (R*)h->l[0];
+    A.vel_out = (R*)h->l[1];
+    A.tm_vel = h->tm[TM_VEL];
+    A.tm_l = h->tm[TM_L1];
+    A.tm_cp = h->tm[TM_CP];
+    A.tm_cv = h->tm[TM_CV];
+    auto set_mode = [&](int m) {
+      A.mode = m;
+      A.phi = m == M_S4 ? (const R*)h->l[2] : (const R*)h->field;
+      A.tm_phi = h->tm[m == M_S4 ? TM_T4 : TM_FIELD];
+      A.out_l = m == M_S1 ? (R*)h->l[0] : m == M_S2 ? (R*)h->l[1] : nullptr;
+      A.with_energy = m == M_S1 ? 1 : 0;
+    };
+    auto time_mode = [&](float& out) -> int {
+      int rc = launch(h, A, true);  // warm-up
+      if (rc) return rc;
+      CK(cudaEventRecord(e0, h->stream));
+      for (int i = 0; i < iters && rc == SS_OK; ++i) rc = launch(h, A, true);
+      CK(cudaEventRecord(e1, h->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      out = ms / iters;
+      return rc;
+    };
     const int modes[4] = {M_S1, M_S2, M_S3, M_S4};
     int rc = SS_OK;
     for (int mi = 0; mi < 4 && rc == SS_OK; ++mi) {
       const int m = modes[mi];
-      A.mode = m;
-      A.out_l = m == M_S1 ? (R*)h->l[0] : m == M_S2 ? (R*)h->l[1] : m == M_S3 ? (R*)h->l[2] : nullptr;
-      A.tm_l = m == M_S3 ? h->tm[4] : h->tm[5];
-      A.with_energy = m == M_S1 ? 1 : 0;
+      if (m == M_S4) {  // stage 4's inputs from this field, whatever stage 3's variants
+        set_mode(M_S3);
+        if ((rc = launch(h, A, true))) break;
+      }
+      set_mode(m);
       if (!uses_pipe(m)) {
         h->use_pipe[m] = 0;
         continue;
       }
       for (int v = 0; v < 2 && rc == SS_OK; ++v) {
         h->use_pipe[m] = v;
-        rc = launch(h, A, true);  // warm-up
-        if (rc) break;
-        CK(cudaEventRecord(e0, h->stream));
-        for (int i = 0; i < iters && rc == SS_OK; ++i) rc = launch(h, A, true);
-        CK(cudaEventRecord(e1, h->stream));
-        CK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
-        h->tune_ms[m][v] = ms / iters;
+        rc = time_mode(h->tune_ms[m][v]);
       }
       h->use_pipe[m] = h->tune_ms[m][1] <= h->tune_ms[m][0] ? 1 : 0;
     }
@@ -622,20 +603,9 @@ struct Fused {
     h->use_pipe[M_GRAD] = h->use_pipe[M_S2];
     // fused stages 2+3 against the two chosen stage kernels
     if (rc == SS_OK) {
-      A.mode = M_S23;
-      A.out_l = (R*)h->l[2];
-      A.out_l2 = (R*)h->l[1];
-      A.tm_l = h->tm[4];
-      A.with_energy = 0;
-      rc = launch(h, A, true);  // warm-up
+      set_mode(M_S23);
+      rc = time_mode(h->tune_ms[M_S23][1]);
       if (rc == SS_OK) {
-        CK(cudaEventRecord(e0, h->stream));
-        for (int i = 0; i < iters && rc == SS_OK; ++i) rc = launch(h, A, true);
-        CK(cudaEventRecord(e1, h->stream));
-        CK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
-        h->tune_ms[M_S23][1] = ms / iters;
         h->tune_ms[M_S23][0] = h->tune_ms[M_S2][h->use_pipe[M_S2]] + h->tune_ms[M_S3][h->use_pipe[M_S3]];
         h->fuse23 = h->tune_ms[M_S23][1] <= h->tune_ms[M_S23][0] ? 1 : 0;
       }
@@ -962,10 +932,10 @@ int ss_bind(ss_handle* h, void* field, void* velocity, void* workspace, size_t w
   h->E_last_host = NAN;
   h->tma = false;
   if (h->precision != SS_PLAIN_FP64 && field && velocity) {
-    const void* bufs[8] = {field, velocity, h->phi_alt, h->vel_alt, h->l[0], h->l[1], h->l[0], h->l[2]};
+    const void* bufs[TM_COUNT] = {field, velocity, h->l[0], h->l[2], h->cp_buf, h->cv_buf};
     bool ok = true;
-    for (int i = 0; i < 8 && ok; ++i)
-      ok = encode_tile_map(&h->tm[i], bufs[i], h->elem, h->G.X, h->G.Y, h->nf, i >= 6);
+    for (int i = 0; i < TM_COUNT && ok; ++i)
+      ok = encode_tile_map(&h->tm[i], bufs[i], h->elem, h->G.X, h->G.Y, h->nf, i >= TM_CP);
     h->tma = ok;
   }
   int dev = 0, sms = 0;
@@ -1568,7 +1538,7 @@ size_t batch_layout(ss_batch* b, char* base) {
     I.partial = (double*)take(sizeof(double) * b->max_tiles[i]);
     I.E_traj = b->d_E ? b->d_E + (size_t)i * TRAJ_CAP : nullptr;
     I.err_traj = b->d_err ? b->d_err + (size_t)i * TRAJ_CAP : nullptr;
-    for (int k = 2; k < 7; ++k) I.buf[k] = take(fb);
+    for (int k = BB_CP; k < BB_COUNT; ++k) I.buf[k] = take(fb);
   }
   return off;
 }
@@ -1612,13 +1582,8 @@ struct Batched {
     BatchStep B;
     memset(&B, 0, sizeof(B));
     B.wait_cycles = b->wait_cycles;
-    int parity = 0, rc;
+    int rc;
     for (int s = 0; s < n; ++s) {
-      // the last step of an odd count ends in the caller's buffers: stage 2 copies phi
-      // and V into the alternates and stage 4 runs at parity 1 (reads the alternates,
-      // writes the caller's buffers), so no copy back follows
-      const bool land = s == n - 1 && parity == 0;
-      B.parity = parity;
       B.with_energy = s > 0;
       B.arrest_update = s > 0;
       B.init_state = s == 0;
@@ -1629,32 +1594,27 @@ struct Batched {
       B.with_energy = B.arrest_update = B.init_state = 0;
       B.prev_energy = nullptr;
       B.E_idx = -1;
-      B.copy_out = land;
       if (b->tma) {  // stages 2 and 3 fused (one staging of phi, V, l1)
         if ((rc = launch<M_S23>(b, B))) return rc;
       } else {
         if ((rc = launch<M_S2>(b, B))) return rc;
-        B.copy_out = 0;
         if ((rc = launch<M_S3>(b, B))) return rc;
       }
-      B.copy_out = 0;
       B.err_idx = s;
-      if (land) B.parity = 1;
-      if ((rc = launch<M_S4>(b, B))) return rc;
+      if ((rc = launch<M_S4>(b, B))) return rc;  // in place
       B.err_idx = -1;
-      if (!land) parity ^= 1;
     }
-    B.parity = parity;
     B.with_energy = B.arrest_update = 1;
     B.E_idx = n - 1;
     if ((rc = launch<M_ENERGY>(b, B))) return rc;
-    batch_finish_kernel<R, TH::NF><<<dim3(64, b->n), 256, 0, b->stream>>>(b->d_insts, parity);
+    batch_finish_kernel<R, TH::NF><<<dim3(64, b->n), 256, 0, b->stream>>>(b->d_insts);
     CK(cudaGetLastError());
     return SS_OK;
   }
 
   // The stage launches of one step with every reduction, trajectory and arrest update
-  // off: reads the current fields, writes only workspace scratch (l1..l3, alternates).
+  // off: reads the current fields, writes only workspace scratch (l1, l2, T4, cV, cP,
+  // and stage 4's phi' and V' into l1 and l2).
   static int timing_step(ss_batch* b) {
     BatchStep B;
     memset(&B, 0, sizeof(B));
@@ -1664,6 +1624,7 @@ struct Batched {
     int rc = launch<M_S1>(b, B);
     if (!rc) rc = b->tma ? launch<M_S23>(b, B) : launch<M_S2>(b, B);
     if (!rc && !b->tma) rc = launch<M_S3>(b, B);
+    B.scratch_out = 1;
     if (!rc) rc = launch<M_S4>(b, B);
     return rc;
   }
@@ -1691,8 +1652,9 @@ bool batch_encode(ss_batch* b, int i) {
   BatchInst& I = b->h_insts[i];
   const int sh = b->shape[i];
   bool ok = true;
-  for (int k = 0; k < 6 && ok; ++k)
-    ok = encode_tile_map(&I.tm[k], I.buf[k], b->elem, I.G.X, I.G.Y, b->nf, false, BSHAPE_TX[sh], BSHAPE_TY[sh]);
+  for (int k = 0; k < BT_COUNT && ok; ++k)
+    ok = encode_tile_map(&I.tm[k], I.buf[BATCH_TM_BUF[k]], b->elem, I.G.X, I.G.Y, b->nf, false, BSHAPE_TX[sh],
+                         BSHAPE_TY[sh]);
   return ok;
 }
 

@@ -11,11 +11,17 @@
 
 namespace ssb {
 
+// a lattice's buffers (BatchInst::buf) and halo-box TMA maps (BatchInst::tm, the
+// buffers BATCH_TM_BUF names)
+enum { BB_FIELD = 0, BB_VEL = 1, BB_CP = 2, BB_CV = 3, BB_L1 = 4, BB_L2 = 5, BB_T4 = 6, BB_COUNT = 7 };
+enum { BT_FIELD = 0, BT_VEL = 1, BT_L1 = 2, BT_T4 = 3, BT_COUNT = 4 };
+constexpr int BATCH_TM_BUF[BT_COUNT] = {BB_FIELD, BB_VEL, BB_L1, BB_T4};
+
 struct BatchInst {
-  CUtensorMap tm[6];  // halo-box TMA maps: field, velocity, phi_alt, vel_alt, l1, l2
+  CUtensorMap tm[BT_COUNT];
   Grid G;
   Phys P;
-  void* buf[7];       // field, velocity, phi_alt, vel_alt, l1, l2, l3
+  void* buf[BB_COUNT];  // field, velocity, cP, cV, l1, l2 (four-kernel steps), T4
   StepState* st;
   double* partial;    // one slot per tile of this lattice
   double* E_traj;     // per-lattice trajectory rows
@@ -24,12 +30,10 @@ struct BatchInst {
 };
 
 struct BatchStep {
-  int parity;         // 0: the caller's buffers hold the current field; 1: the alternates do
-  int copy_out;       // S2 / M_S23 at parity 0: also copy phi's and V's centres into the
-                      // alternates (the last step of an odd count; its S4 runs at parity 1)
   int with_energy, arrest_update, init_state;
   int E_idx, err_idx;
   const double* prev_energy;  // device, one per lattice (NaN keeps E_last); read with init_state
+  int scratch_out;            // stage 4 writes phi' and V' into l1 and l2 (timing)
   long long wait_cycles;
 };
 
@@ -52,10 +56,9 @@ __global__ void __launch_bounds__(NT, (batch_ctas<R, MODE, NT>()))
   __shared__ FlowArgs<R> A;
   const int inst = tile_inst[blockIdx.x];
   const BatchInst& I = insts[inst];
-  const int cur = B.parity;
-  const CUtensorMap* tm_phi = &I.tm[cur ? 2 : 0];
-  const CUtensorMap* tm_vel = &I.tm[cur ? 3 : 1];
-  const CUtensorMap* tm_l = &I.tm[(MODE == M_S3 || MODE == M_S23) ? 4 : 5];
+  const CUtensorMap* tm_phi = &I.tm[MODE == M_S4 ? BT_T4 : BT_FIELD];
+  const CUtensorMap* tm_vel = &I.tm[BT_VEL];
+  const CUtensorMap* tm_l = &I.tm[BT_L1];
   if constexpr (TMA) {
     // the tile's loads first, so the set-up below overlaps them
     if (threadIdx.x == 0) {
@@ -75,20 +78,19 @@ __global__ void __launch_bounds__(NT, (batch_ctas<R, MODE, NT>()))
     for (int i = threadIdx.x; i < (int)(sizeof(Phys) / 4); i += NT) dst[i] = src[i];
   }
   if (threadIdx.x == 0) {
-    A.phi = (const R*)I.buf[cur ? 2 : 0];
-    A.vel = (const R*)I.buf[cur ? 3 : 1];
-    A.la = (const R*)I.buf[4];
-    A.lb = (const R*)I.buf[5];
-    A.lc = (const R*)I.buf[6];
-    A.out_l = MODE == M_S1 ? (R*)I.buf[4] : MODE == M_S2 ? (R*)I.buf[5] : (MODE == M_S3 || MODE == M_S23)
-                                                                            ? (R*)I.buf[6] : nullptr;
-    A.out_l2 = MODE == M_S23 ? (R*)I.buf[5] : nullptr;
+    A.phi = (const R*)I.buf[MODE == M_S4 ? BB_T4 : BB_FIELD];
+    A.vel = (const R*)I.buf[BB_VEL];
+    A.la = (const R*)I.buf[BB_L1];
+    A.lb = (const R*)I.buf[BB_L2];
+    A.cp = (const R*)I.buf[BB_CP];
+    A.cv = (const R*)I.buf[BB_CV];
+    A.out_l = MODE == M_S1 ? (R*)I.buf[BB_L1] : MODE == M_S2 ? (R*)I.buf[BB_L2] : nullptr;
+    A.out_t4 = (R*)I.buf[BB_T4];
+    A.out_cp = (R*)I.buf[BB_CP];
+    A.out_cv = (R*)I.buf[BB_CV];
     A.out_eg = nullptr;
-    A.phi_out = (R*)I.buf[cur ? 0 : 2];
-    A.vel_out = (R*)I.buf[cur ? 1 : 3];
-    const bool copy = (MODE == M_S2 || MODE == M_S23) && B.copy_out;
-    A.copy_phi = copy ? (R*)I.buf[2] : nullptr;
-    A.copy_vel = copy ? (R*)I.buf[3] : nullptr;
+    A.phi_out = (R*)I.buf[B.scratch_out ? BB_L1 : BB_FIELD];
+    A.vel_out = (R*)I.buf[B.scratch_out ? BB_L2 : BB_VEL];
     A.force = nullptr;
     A.partial = I.partial;
     A.st = I.st;
@@ -110,23 +112,16 @@ __global__ void __launch_bounds__(NT, (batch_ctas<R, MODE, NT>()))
   flow_tile<TH, R, TX, TY, NT, TMA, MODE>(A, tm_phi, tm_vel, tm_l, blockIdx.x - I.tile0, I.ntiles, smem_raw, S, TMA);
 }
 
-// Copy each lattice's result back into the caller's buffers when the alternates hold
-// it, and apply a pending arrest (V = 0).  grid.y = lattice.
+// Apply each lattice's pending arrest (V = 0), left by the trailing energy pass, at the
+// end of a call.  grid.y = lattice.
 template <typename R, int NF>
-__global__ void batch_finish_kernel(const BatchInst* __restrict__ insts, int parity) {
+__global__ void batch_finish_kernel(const BatchInst* __restrict__ insts) {
   const BatchInst& I = insts[blockIdx.y];
-  const bool arrest = I.st->arrest != 0;
-  const bool copy = parity != 0;
-  if (!copy && !arrest) return;
-  R* dp = (R*)I.buf[0];
-  R* dv = (R*)I.buf[1];
-  const R* sp = (const R*)I.buf[2];
-  const R* sv = (const R*)I.buf[3];
+  if (I.st->arrest == 0) return;
+  R* dv = (R*)I.buf[BB_VEL];
   const long long n = (long long)NF * I.G.N;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    if (copy) dp[i] = sp[i];
-    dv[i] = arrest ? (R)0 : (copy ? sv[i] : dv[i]);
-  }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dv[i] = (R)0;
 }
 
 }  // namespace ssb

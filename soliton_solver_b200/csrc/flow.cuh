@@ -7,18 +7,22 @@
 //   k4 = dt (V + l3),     T4 = phi + k3,      l4 = -dt G(T4)
 //   V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,  phi' = phi + (k1 + 2 k2 + 2 k3 + k4)/6
 // followed by the unit-norm re-projection, the energy of phi', the arrest test
-// (E' > E -> V' = 0) and err = max G(T4).  Here every k_s and T_s is recomputed from
-// (phi, V, l_s) while a tile is staged, so stage s reads only what it needs:
-//   S1 reads phi                       writes l1  (+ energy of phi, see below)
-//   S2 reads phi, V                    writes l2
-//   S3 reads phi, V, l1                writes l3
-//   S4 reads phi, V, l1, l2, l3        writes phi', V' (ping-pong buffers), err
-// The energy of a step's result is computed by the NEXT step's S1, which stages
-// exactly that field anyway, and the arrest decision is kept on the device
-// (StepState.arrest) and applied by S2..S4 as "V = 0".  A trailing energy pass
-// closes a call.  Compulsory traffic: 16 words per site and step as four kernels
-// (S1 2, S2 3, S3 4, S4 7); 14 when stages 2 and 3 run as one kernel (M_S23), which
-// stages phi, V and l1 once and writes l2 and l3.
+// (E' > E -> V' = 0) and err = max G(T4).  The update is linear in V and the l_s, so
+// everything stage 4 needs besides l4 is known once l2 and l3 are:
+//   T4 = phi + dt (V + l2/2),  cV = V + (l1 + 2 l2 + 2 l3)/6,  cP = phi + dt V + dt (l1 + l2 + l3)/6
+//   V' = cV + l4/6,            phi' = cP (re-projected)
+// Stage s recomputes its T_s from (phi, V, l_s) while a tile is staged:
+//   S1  reads phi                        writes l1  (+ energy of phi, see below)
+//   S2  reads phi, V                     writes l2
+//   S3  reads phi, V, l1 (+ l2 centres)  writes T4, cV, cP
+//   S4  reads T4 (halo tile), cP, cV     writes phi', V', err
+// Stage 4 reads neither phi nor V, so it writes the caller's buffers in place (no
+// ping-pong copies).  The energy of a step's result is computed by the NEXT step's S1,
+// which stages exactly that field anyway, and the arrest decision is kept on the
+// device (StepState.arrest) and applied by S2/S3 as "V = 0".  A trailing energy pass
+// closes a call.  Compulsory traffic: 13 words per site and step when stages 2 and 3
+// run as one kernel (M_S23: S1 2, S2+S3 6, S4 5), 17 as four kernels (S2 3, S3 7 with
+// the l2 centres).
 #pragma once
 
 #include <cuda.h>
@@ -41,23 +45,24 @@ constexpr long long WAIT_CYCLES = 2000000000LL;
 
 template <typename R>
 struct FlowArgs {
-  CUtensorMap tm_phi;  // TMA maps (used when the kernel is instantiated with TMA)
-  CUtensorMap tm_vel;
-  CUtensorMap tm_l;    // l1 (S3) or l2 (S4)
-  CUtensorMap tm_c1;   // l1 centre tiles (pipelined S4)
-  CUtensorMap tm_c3;   // l3 centre tiles (pipelined S4)
-  const R* phi;
-  const R* vel;
-  const R* la;  // l1 (S3, S4)
-  const R* lb;  // l2 (S4)
-  const R* lc;  // l3 (S4)
-  R* out_l;     // S1..S3: l_s;  M_S23: l3;  M_GRAD: l_out (nullable)
-  R* out_l2;    // M_S23: l2
-  R* out_eg;    // M_GRAD: energy gradient (nullable)
-  R* phi_out;   // S4
-  R* vel_out;   // S4
-  R* copy_phi;  // S2 / M_S23, one tile per CTA (nullable): copy of phi's and V's centres, so
-  R* copy_vel;  //   that this step's S4 can read them there and write into phi / vel
+  CUtensorMap tm_phi;  // TMA maps (used when the kernel is instantiated with TMA):
+  CUtensorMap tm_vel;  //   halo boxes of the staged field (phi; T4 in S4), of V,
+  CUtensorMap tm_l;    //   of l1 (S3, M_S23),
+  CUtensorMap tm_cp;   //   and centre boxes of cP and cV (pipelined S4)
+  CUtensorMap tm_cv;
+  const R* phi;  // the staged field: phi, or T4 in S4
+  const R* vel;  // V (S2, S3, M_S23)
+  const R* la;   // l1 (S3, M_S23)
+  const R* lb;   // l2 (S3)
+  const R* cp;   // S4: cP = phi + dt V + dt (l1 + l2 + l3)/6
+  const R* cv;   // S4: cV = V + (l1 + 2 l2 + 2 l3)/6
+  R* out_l;      // S1, S2: l_s;  M_GRAD: l_out (nullable)
+  R* out_t4;     // S3 / M_S23: T4 = phi + dt (V + l2/2)
+  R* out_cp;     // S3 / M_S23: cP
+  R* out_cv;     // S3 / M_S23: cV
+  R* out_eg;     // M_GRAD: energy gradient (nullable)
+  R* phi_out;    // S4: phi' (may be the caller's phi: stage 4 reads neither phi nor V)
+  R* vel_out;    // S4: V'
   const double* force;  // FP64 fields (nullable): added to the flow's gradient rows in every stage
   double* partial;  // per-block energy partials
   StepState* st;
@@ -92,58 +97,14 @@ struct TileShape {
   static_assert(TY % 4 == 0, "TY must keep the y start 16-byte aligned");
 };
 
-// Centre of a tile (TX x TY sites, NF components) of phi and V into A.copy_phi /
-// A.copy_vel (each skipped when null), from the staged halo tiles Pt / Vt (phi and V
-// as loaded) or, when those are null, from A.phi / A.vel.  Lattice rows whose length
-// is a multiple of 16 bytes (always so under TMA staging) copy 16-byte vectors: staged
-// rows start 16-byte aligned (the pitch and the y offset are multiples of 16 bytes).
-template <int NF, typename R, int TX, int TY, int NT, typename FA>
-__device__ __forceinline__ void copy_centre(const FA& A, const R* Pt, const R* Vt, int x0, int y0) {
-  using TS = TileShape<TX, TY, NT>;
-  const Grid& G = A.G;
-  constexpr int VW = 16 / sizeof(R);  // elements per 16-byte vector
-  static_assert(TY % VW == 0 && (TS::HY * sizeof(R)) % 16 == 0 && (TS::YOFF * sizeof(R)) % 16 == 0, "alignment");
-  auto al16 = [](const void* q) { return ((uintptr_t)q & 15u) == 0; };  // null counts as aligned
-  // rows of whole vectors, and every base pointer involved 16-byte aligned (the caller's
-  // buffers need not be under plain staging); uniform over the block
-  const bool vec = G.Y % VW == 0 && al16(A.copy_phi) && al16(A.copy_vel) && (Pt || !A.copy_phi || al16(A.phi)) &&
-                   (Vt || !A.copy_vel || al16(A.vel));
-  if (vec) {
-    constexpr int RV = TY / VW;  // vectors per tile row
-#pragma unroll 2
-    for (int i = threadIdx.x; i < NF * TX * RV; i += NT) {
-      const int yv = i % RV, lx = (i / RV) % TX, a = i / (TX * RV);
-      const int gx = x0 + lx, gy = y0 + yv * VW;
-      if (gx >= G.X || gy >= G.Y) continue;
-      const long long g = a * G.N + (long long)gx * G.Y + gy;
-      const int t = a * TS::PLANE + (lx + 2) * TS::HY + TS::YOFF + yv * VW;
-      if (A.copy_phi)
-        *reinterpret_cast<uint4*>(A.copy_phi + g) = *reinterpret_cast<const uint4*>(Pt ? Pt + t : A.phi + g);
-      if (A.copy_vel)
-        *reinterpret_cast<uint4*>(A.copy_vel + g) = *reinterpret_cast<const uint4*>(Vt ? Vt + t : A.vel + g);
-    }
-    return;
-  }
-#pragma unroll 4
-  for (int i = threadIdx.x; i < NF * TX * TY; i += NT) {
-    const int y = i % TY, lx = (i / TY) % TX, a = i / (TX * TY);
-    const int gx = x0 + lx, gy = y0 + y;
-    if (gx >= G.X || gy >= G.Y) continue;
-    const long long g = a * G.N + (long long)gx * G.Y + gy;
-    const int t = a * TS::PLANE + (lx + 2) * TS::HY + TS::YOFF + y;
-    if (A.copy_phi) A.copy_phi[g] = Pt ? Pt[t] : A.phi[g];
-    if (A.copy_vel) A.copy_vel[g] = Vt ? Vt[t] : A.vel[g];
-  }
-}
-
 template <typename R, int NF, int TX, int TY>
 __host__ __device__ constexpr size_t tile_buf_bytes() {
   return sizeof(R) * NF * (TX + 4) * (TY + 8);
 }
 
-// number of staged buffers a mode needs (phi, then velocity, then l)
+// number of staged halo buffers a mode needs (phi, then V, then l1; T4 alone in S4)
 __host__ __device__ constexpr int flow_buffers(int mode) {
-  return mode == M_S2 ? 2 : (mode == M_S3 || mode == M_S4 || mode == M_S23) ? 3 : 1;
+  return mode == M_S2 ? 2 : (mode == M_S3 || mode == M_S23) ? 3 : 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -187,25 +148,24 @@ __device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long lo
 }
 
 // T_s for one element from the staged inputs (the reference's k / Temp algebra,
-// core/integrator.py:51-96 and :323-334)
+// core/integrator.py:51-96 and :323-334); stage 4's T4 is stored by stage 3
 template <typename R>
 __device__ inline R stage_value(int mode, R p, R v, R w, R dt) {
   const R half = (R)0.5;
   if (mode == M_S2) return p + half * (dt * v);
   if (mode == M_S3) return p + half * (dt * (v + half * w));
-  if (mode == M_S4) return p + dt * (v + half * w);
   return p;
 }
 
-// Plain-load staging of T_s into `T` (all components), used when a TMA map cannot
-// describe the buffers (row pitch not a multiple of 16 bytes).  Every thread first
-// issues all loads of one component plane, then combines and stores, so each
-// plane costs one memory round trip.
+// Plain-load staging of one halo buffer T = T_s(psrc, vsrc, wsrc) (all components;
+// vsrc / wsrc nullable), used when a TMA map cannot describe the buffers (row pitch
+// not a multiple of 16 bytes).  Every thread first issues all loads of one component
+// plane, then combines and stores, so each plane costs one memory round trip.
 template <int NF, typename R, int TX, int TY, int NT>
-__device__ inline void stage_plain(R* T, const FlowArgs<R>& A, int x0, int y0, int mode, bool arrest) {
+__device__ inline void stage_plain_buf(R* T, const Grid& G, const R* psrc, const R* vsrc, const R* wsrc, int x0,
+                                       int y0, int mode) {
   using TS = TileShape<TX, TY, NT>;
   constexpr int KM = (TS::PLANE + NT - 1) / NT;
-  const Grid& G = A.G;
   const long long N = G.N;
   const R dt = (R)G.dt;
   long long off[KM];
@@ -218,17 +178,15 @@ __device__ inline void stage_plain(R* T, const FlowArgs<R>& A, int x0, int y0, i
     ok[k] = i < TS::PLANE && gx >= 0 && gx < G.X && gy >= 0 && gy < G.Y;
     off[k] = (long long)gx * G.Y + gy;
   }
-  const bool need_v = (mode == M_S2 || mode == M_S3 || mode == M_S4) && !arrest;
-  const R* lsrc = mode == M_S3 ? A.la : (mode == M_S4 ? A.lb : nullptr);
 #pragma unroll
   for (int a = 0; a < NF; ++a) {
     R p[KM], v[KM], w[KM];
     const long long base = (long long)a * N;
 #pragma unroll
     for (int k = 0; k < KM; ++k) {
-      p[k] = ok[k] ? A.phi[base + off[k]] : (R)0;
-      v[k] = (ok[k] && need_v) ? A.vel[base + off[k]] : (R)0;
-      w[k] = (ok[k] && lsrc) ? lsrc[base + off[k]] : (R)0;
+      p[k] = ok[k] ? psrc[base + off[k]] : (R)0;
+      v[k] = (ok[k] && vsrc) ? vsrc[base + off[k]] : (R)0;
+      w[k] = (ok[k] && wsrc) ? wsrc[base + off[k]] : (R)0;
     }
 #pragma unroll
     for (int k = 0; k < KM; ++k) {
@@ -236,6 +194,32 @@ __device__ inline void stage_plain(R* T, const FlowArgs<R>& A, int x0, int y0, i
       if (i < TS::PLANE) T[a * TS::PLANE + i] = stage_value<R>(mode, p[k], v[k], w[k], dt);
     }
   }
+}
+
+// Plain-load staging of T_s into T (T4, stored by stage 3, in S4)
+template <int NF, typename R, int TX, int TY, int NT>
+__device__ inline void stage_plain(R* T, const FlowArgs<R>& A, int x0, int y0, int mode, bool arrest) {
+  const bool need_v = (mode == M_S2 || mode == M_S3) && !arrest;
+  stage_plain_buf<NF, R, TX, TY, NT>(T, A.G, A.phi, need_v ? A.vel : nullptr, mode == M_S3 ? A.la : nullptr, x0, y0,
+                                     mode);
+}
+
+// The unit-norm re-projection of a site pair's magnetisation components
+// (compute_norm_magnetization, chiral_magnet/kernels.py:48-84): m / |m| where |m| > 0.
+template <int NMAG, typename V>
+__device__ __forceinline__ void unit_project(V* m) {
+  using S = typename ScalarOf<V>::type;
+  V s2 = m[0] * m[0];
+#pragma unroll
+  for (int a = 1; a < NMAG; ++a) s2 = vfma(m[a], m[a], s2);
+  V inv(1.0);
+#pragma unroll
+  for (int l = 0; l < 2; ++l) {
+    const S s = sqrt(Lanes<V>::get(s2, l));
+    if (s != (S)0) Lanes<V>::set(inv, l, (S)1 / s);
+  }
+#pragma unroll
+  for (int a = 0; a < NMAG; ++a) m[a] = m[a] * inv;
 }
 
 // Stencil weights pre-scaled by the lattice spacings, as broadcast pairs.
@@ -359,16 +343,62 @@ __device__ __forceinline__ double jet_energy(const Jet<V, NF>& J, const Phys& P,
   return e;
 }
 
+// Jet of every component of the site pair whose centre starts at `toff` in the staged
+// halo buffer T (NF planes of PLANE values), with the derivative masks applied.
+template <class TH, typename V, typename R, int HY, int PLANE, bool FAST>
+__device__ __forceinline__ void tile_jet(const R* T, int toff, const PairCoef<V>& kc, const Masks& m0, const Masks& m1,
+                                         Jet<V, TH::NF>& J) {
+#pragma unroll
+  for (int a = 0; a < TH::NF; ++a) {
+    V Dx1, Dx2, Dy1, Dy2;
+    pair_jet<V, R, HY, TH::NEED_XY>(T + a * PLANE + toff, kc, J.f[a], J.dx[a], J.dy[a], J.dxx[a], J.dyy[a], J.dxy[a],
+                                    Dx1, Dx2, Dy1, Dy2);
+    if (!FAST) {
+      J.dx[a] = mask_lanes(J.dx[a], m0.x, m1.x);
+      J.dy[a] = mask_lanes(J.dy[a], m0.y, m1.y);
+      J.dxx[a] = mask_lanes(J.dxx[a], m0.x, m1.x);
+      J.dyy[a] = mask_lanes(J.dyy[a], m0.y, m1.y);
+      J.dxy[a] = mask_lanes(J.dxy[a], m0.xy, m1.xy);
+    }
+  }
+}
+
+// The flow's constraints on a site pair's gradient rows: zero on the frozen ring
+// (theories with HALO_ZERO) and the tangent projection g - (g . m) m
+// (project_orthogonal_magnetization, chiral_magnet/kernels.py:86-122).
+template <class TH, typename V, bool FAST>
+__device__ __forceinline__ void flow_constraints(const Grid& G, const Jet<V, TH::NF>& J, V* g, int gx, int gy) {
+  if (TH::HALO_ZERO && !FAST) {
+    const bool e0 = gx < G.halo || gx > G.X - G.halo - 1 || gy < G.halo || gy > G.Y - G.halo - 1;
+    const bool e1 = gx < G.halo || gx > G.X - G.halo - 1 || gy + 1 < G.halo || gy + 1 > G.Y - G.halo - 1;
+#pragma unroll
+    for (int a = 0; a < TH::NF; ++a) g[a] = mask_lanes(g[a], !e0, !e1);
+  }
+  if (TH::CONSTRAINED) {
+    V lm = g[0] * J.f[0];
+#pragma unroll
+    for (int a = 1; a < TH::NMAG; ++a) lm = vfma(g[a], J.f[a], lm);
+    const V mlm = -lm;
+#pragma unroll
+    for (int a = 0; a < TH::NMAG; ++a) g[a] = vfma(mlm, J.f[a], g[a]);
+  }
+}
+
 // The per-site work of one staged tile.  Each thread owns y-adjacent site pairs;
 // FAST: the tile is interior (every derivative mask true, no halo site) and the
 // lattice row length is even, so pairs are aligned and need no lane masks.
+//   T      the staged stencil field: T1 (S1, M_GRAD, M_ENERGY), T2 (S2), T3 (S3, M_S23), T4 (S4)
+//   T2     M_S23: the staged T2 (l2 and l3 of a pair are computed in one pass)
+//   Praw   S3 / M_S23: the staged phi (else phi is read from A.phi)
+//   Vraw   S3: the staged V (else V is read from A.vel); unused when arrested
+//   Cp, Cv S4: the staged cP and cV centre tiles (else read from A.cp, A.cv)
 // JE (FP32 stage 1 and the energy pass): add the energy of the jets to *e_acc (when
 // non-null); in M_ENERGY the gradient itself is skipped.
 template <class TH, typename R, int TX, int TY, int NT, bool FAST, int MODE, bool JE = false>
-__device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, const R* Praw, const R* Vraw, int x0,
-                                          int y0, bool arrest, double& err_max, const R* C1 = nullptr,
-                                          const R* C3 = nullptr, double* e_acc = nullptr,
-                                          const typename PairOf<R>::type* L2c = nullptr, R* out_l = nullptr) {
+__device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, int x0, int y0, bool arrest,
+                                          double& err_max, double* e_acc = nullptr, const R* Praw = nullptr,
+                                          const R* Vraw = nullptr, const R* T2 = nullptr, const R* Cp = nullptr,
+                                          const R* Cv = nullptr, R* out_l = nullptr) {
   using TS = TileShape<TX, TY, NT>;
   using V = typename PairOf<R>::type;
   constexpr int NF = TH::NF;
@@ -385,9 +415,9 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
   double e_pair = 0.0;
   const int j = threadIdx.x % PAIRS;
   const int lxg = threadIdx.x / PAIRS;
-  // stage 1 and the energy pass (which must reduce alike) give each thread adjacent rows;
-  // the energy pass unrolls them so that the rows share their x-neighbour loads
-  constexpr bool ADJ = JE && (MODE == M_S1 || MODE == M_ENERGY);
+  // stage 1 and the FP32 energy pass give each thread adjacent rows; the energy pass
+  // unrolls them so that the rows share their x-neighbour loads
+  constexpr bool ADJ = sizeof(R) == 4 && (MODE == M_S1 || MODE == M_ENERGY);
 #pragma unroll((JE && MODE == M_ENERGY) ? 2 : 1)
   for (int pass = 0; pass < TX / RPP; ++pass) {
     const int lx = ADJ ? lxg * (TX / RPP) + pass : lxg + pass * RPP;
@@ -405,19 +435,7 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
     const long long sidx = (long long)gx * G.Y + gy;
 
     Jet<V, NF> J;
-    V Dx1[NF], Dx2[NF], Dy1[NF], Dy2[NF];
-#pragma unroll
-    for (int a = 0; a < NF; ++a) {
-      pair_jet<V, R, TS::HY, TH::NEED_XY>(T + a * TS::PLANE + toff, kc, J.f[a], J.dx[a], J.dy[a], J.dxx[a],
-                                                  J.dyy[a], J.dxy[a], Dx1[a], Dx2[a], Dy1[a], Dy2[a]);
-      if (!FAST) {
-        J.dx[a] = mask_lanes(J.dx[a], m0.x, m1.x);
-        J.dy[a] = mask_lanes(J.dy[a], m0.y, m1.y);
-        J.dxx[a] = mask_lanes(J.dxx[a], m0.x, m1.x);
-        J.dyy[a] = mask_lanes(J.dyy[a], m0.y, m1.y);
-        J.dxy[a] = mask_lanes(J.dxy[a], m0.xy, m1.xy);
-      }
-    }
+    tile_jet<TH, V, R, TS::HY, TS::PLANE, FAST>(T, toff, kc, m0, m1, J);
     if constexpr (JE) {
       if (e_acc) {
         if constexpr (TH::PAIR_ENERGY) {
@@ -432,18 +450,22 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
     }
     if constexpr (MODE == M_ENERGY) continue;
 
+    // FP64 fields: a fixed field added to the flow's gradient rows (ss_set_forcing); uniform
+    auto add_force = [&](V* g) {
+      if constexpr (sizeof(R) == 8 && MODE != M_GRAD) {
+        if (A.force) {
+          V fo[NF];
+#pragma unroll
+          for (int a = 0; a < NF; ++a) fo[a] = gload<V, double>(A.force + a * N + sidx, FAST, v1);
+          TH::flow_rows(fo, A.P);
+#pragma unroll
+          for (int a = 0; a < NF; ++a) g[a] = g[a] + fo[a];
+        }
+      }
+    };
     V g[NF];
     TH::gradient(J, A.P, g);
-    if constexpr (sizeof(R) == 8 && MODE != M_GRAD) {
-      if (A.force) {  // uniform: a fixed field added to the flow's gradient (ss_set_forcing)
-        V fo[NF];
-#pragma unroll
-        for (int a = 0; a < NF; ++a) fo[a] = gload<V, double>(A.force + a * N + sidx, FAST, v1);
-        TH::flow_rows(fo, A.P);
-#pragma unroll
-        for (int a = 0; a < NF; ++a) g[a] = g[a] + fo[a];
-      }
-    }
+    add_force(g);
     if constexpr (MODE == M_GRAD) {
       if (A.grad_raw) {
         // functional derivative of the energy: no halo zeroing, no projection, and
@@ -456,63 +478,64 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, cons
         continue;
       }
     }
-    if (TH::HALO_ZERO && !FAST) {
-      const bool e0 = gx < G.halo || gx > G.X - G.halo - 1 || gy < G.halo || gy > G.Y - G.halo - 1;
-      const bool e1 = gx < G.halo || gx > G.X - G.halo - 1 || gy + 1 < G.halo || gy + 1 > G.Y - G.halo - 1;
-#pragma unroll
-      for (int a = 0; a < NF; ++a) g[a] = mask_lanes(g[a], !e0, !e1);
-    }
-    if (TH::CONSTRAINED) {  // project_orthogonal_magnetization (chiral_magnet/kernels.py:86-122)
-      V lm = g[0] * J.f[0];
-#pragma unroll
-      for (int a = 1; a < TH::NMAG; ++a) lm = vfma(g[a], J.f[a], lm);
-      const V mlm = -lm;
-#pragma unroll
-      for (int a = 0; a < TH::NMAG; ++a) g[a] = vfma(mlm, J.f[a], g[a]);
-    }
+    flow_constraints<TH, V, FAST>(G, J, g, gx, gy);
     if constexpr (MODE == M_GRAD) {
 #pragma unroll
       for (int a = 0; a < NF; ++a) {
         if (A.out_eg) gstore<V, R>(A.out_eg + a * N + sidx, g[a], FAST, v1);
         if (A.out_l) gstore<V, R>(A.out_l + a * N + sidx, mdt * g[a], FAST, v1);
       }
-    } else if constexpr (MODE != M_S4) {
+    } else if constexpr (MODE == M_S1 || MODE == M_S2) {
       R* const lo = out_l ? out_l : A.out_l;
 #pragma unroll
       for (int a = 0; a < NF; ++a) gstore<V, R>(lo + a * N + sidx, mdt * g[a], FAST, v1);
-    } else {
-      // RK4 finalize (core/integrator.py:151-189) fused with stage 4:
-      // V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,  phi' = phi + dt V + dt (l1 + l2 + l3)/6
-      V Pn[NF], Vn[NF];
-      const V sixth(grid_k<S>(G, GK_SIXTH)), two(2.0), dtv(grid_k<S>(G, GK_DT)), dt6(grid_k<S>(G, GK_DT6));
+    } else if constexpr (MODE == M_S3 || MODE == M_S23) {
+      // l3 from T3; l2 from T2 (M_S23) or the stored l2 (S3); then the stage-4 inputs
+      // T4 = phi + dt (V + l2/2), cV = V + (l1 + 2 l2 + 2 l3)/6, cP = phi + dt V + dt (l1 + l2 + l3)/6
+      // (core/integrator.py:151-189 with k1 = dt V, k2 = dt (V + l1/2), k3 = dt (V + l2/2))
+      V l2[NF];
+      if constexpr (MODE == M_S23) {
+        Jet<V, NF> J2;
+        tile_jet<TH, V, R, TS::HY, TS::PLANE, FAST>(T2, toff, kc, m0, m1, J2);
+        TH::gradient(J2, A.P, l2);
+        add_force(l2);
+        flow_constraints<TH, V, FAST>(G, J2, l2, gx, gy);
+#pragma unroll
+        for (int a = 0; a < NF; ++a) l2[a] = mdt * l2[a];
+      } else {
+#pragma unroll
+        for (int a = 0; a < NF; ++a) l2[a] = gload<V, R>(A.lb + a * N + sidx, FAST, v1);
+      }
+      const V half(0.5), sixth(grid_k<S>(G, GK_SIXTH)), two(2.0), dtv(grid_k<S>(G, GK_DT)),
+          dt6(grid_k<S>(G, GK_DT6));
 #pragma unroll
       for (int a = 0; a < NF; ++a) {
         const long long idx = a * N + sidx;
         const V p = Praw ? ld_pair(Praw + a * TS::PLANE + toff) : gload<V, R>(A.phi + idx, FAST, v1);
         const V v = arrest ? V(0.0) : (Vraw ? ld_pair(Vraw + a * TS::PLANE + toff) : gload<V, R>(A.vel + idx, FAST, v1));
+        const V l1 = gload<V, R>(A.la + idx, FAST, v1);
+        const V l3 = mdt * g[a];
+        gstore<V, R>(A.out_t4 + idx, vfma(dtv, vfma(half, l2[a], v), p), FAST, v1);
+        gstore<V, R>(A.out_cv + idx, vfma(sixth, vfma(two, l3, vfma(two, l2[a], l1)), v), FAST, v1);
+        gstore<V, R>(A.out_cp + idx, vfma(dt6, (l1 + l2[a]) + l3, vfma(dtv, v, p)), FAST, v1);
+      }
+    } else {
+      // S4: V' = cV + l4/6 and phi' = cP, re-projected onto the sphere, then V' projected
+      // onto the tangent space of phi' (compute_norm_magnetization and
+      // project_orthogonal_magnetization, chiral_magnet/kernels.py:48-122)
+      V Pn[NF], Vn[NF];
+      const V sixth(grid_k<S>(G, GK_SIXTH));
+#pragma unroll
+      for (int a = 0; a < NF; ++a) {
         const int coff = a * TX * TY + lx * TY + 2 * j;
-        const V l1 = C1 ? ld_pair(C1 + coff) : gload<V, R>(A.la + idx, FAST, v1);
-        const V l2 = L2c ? L2c[a] : gload<V, R>(A.lb + idx, FAST, v1);
-        const V l3 = C3 ? ld_pair(C3 + coff) : gload<V, R>(A.lc + idx, FAST, v1);
-        const V l4 = mdt * g[a];
-        Vn[a] = vfma(sixth, vfma(two, l3, vfma(two, l2, l1)) + l4, v);
-        Pn[a] = vfma(dt6, (l1 + l2) + l3, vfma(dtv, v, p));
+        const V cv = Cv ? ld_pair(Cv + coff) : gload<V, R>(A.cv + a * N + sidx, FAST, v1);
+        Pn[a] = Cp ? ld_pair(Cp + coff) : gload<V, R>(A.cp + a * N + sidx, FAST, v1);
+        Vn[a] = vfma(sixth, mdt * g[a], cv);
         emax = fmax(emax, Lanes<V>::get(g[a], 0));
         if (v1) emax = fmax(emax, Lanes<V>::get(g[a], 1));
       }
       if (TH::CONSTRAINED && G.unit_mag) {
-        // compute_norm_magnetization + project_orthogonal_magnetization (kernels.py:48-122)
-        V s2 = Pn[0] * Pn[0];
-#pragma unroll
-        for (int a = 1; a < TH::NMAG; ++a) s2 = vfma(Pn[a], Pn[a], s2);
-        V inv(1.0);
-#pragma unroll
-        for (int l = 0; l < 2; ++l) {
-          const S s = sqrt(Lanes<V>::get(s2, l));
-          if (s != (S)0) Lanes<V>::set(inv, l, (S)1 / s);
-        }
-#pragma unroll
-        for (int a = 0; a < TH::NMAG; ++a) Pn[a] = Pn[a] * inv;
+        unit_project<TH::NMAG>(Pn);
         V lm = Vn[0] * Pn[0];
 #pragma unroll
         for (int a = 1; a < TH::NMAG; ++a) lm = vfma(Vn[a], Pn[a], lm);
@@ -593,23 +616,22 @@ __device__ __forceinline__ double energy_tile(const FlowArgs<R>& A, const E* T, 
   return e_acc + (double)(Lanes<V>::get(chk, 0) + Lanes<V>::get(chk, 1));
 }
 
-// Expect and issue the TMA loads of one tile's staged buffers (called by one thread,
-// after the barrier is initialised): phi into B0, and V into B0 + BUF and the mode's l
-// buffer into B0 + 2 BUF where the mode combines them.  V is staged whether or not an
-// arrest is pending (an arrested step ignores it).
+// Expect and issue the TMA loads of one tile's staged halo buffers (called by one
+// thread, after the barrier is initialised): tm_phi into B0 (phi; T4 in S4), then V
+// into B0 + BUF in S2, S3 and M_S23 and l1 into B0 + 2 BUF in S3 and M_S23.  V is
+// staged whether or not an arrest is pending (an arrested step ignores it).
 template <class TH, typename R, int TX, int TY, int NT, int MODE>
 __device__ __forceinline__ void issue_tile(R* B0, const CUtensorMap* tm_phi, const CUtensorMap* tm_vel,
                                            const CUtensorMap* tm_l, int x0, int y0, uint64_t* bar,
                                            unsigned tx_extra) {
   using TS = TileShape<TX, TY, NT>;
   constexpr int BUF = TH::NF * TS::PLANE;
-  constexpr bool need_v = MODE == M_S2 || MODE == M_S3 || MODE == M_S4 || MODE == M_S23;
-  constexpr bool need_l = MODE == M_S3 || MODE == M_S4 || MODE == M_S23;
-  constexpr uint32_t bytes = (uint32_t)(sizeof(R) * BUF) * (1u + (need_v ? 1u : 0u) + (need_l ? 1u : 0u));
+  constexpr int NB = flow_buffers(MODE);
+  constexpr uint32_t bytes = (uint32_t)(sizeof(R) * BUF) * (uint32_t)NB;
   mbar_expect_tx(bar, bytes + tx_extra);
   tma_load_3d(B0, tm_phi, y0 - TS::YOFF, x0 - 2, 0, bar);
-  if constexpr (need_v) tma_load_3d(B0 + BUF, tm_vel, y0 - TS::YOFF, x0 - 2, 0, bar);
-  if constexpr (need_l) tma_load_3d(B0 + 2 * BUF, tm_l, y0 - TS::YOFF, x0 - 2, 0, bar);
+  if constexpr (NB >= 2) tma_load_3d(B0 + BUF, tm_vel, y0 - TS::YOFF, x0 - 2, 0, bar);
+  if constexpr (NB >= 3) tma_load_3d(B0 + 2 * BUF, tm_l, y0 - TS::YOFF, x0 - 2, 0, bar);
 }
 
 // Shared scratch of the one-tile-per-CTA stage kernels besides the staged tile.
@@ -642,12 +664,11 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   int& am_last = S.am_last;
 
   const Grid& G = A.G;
-  constexpr int mode = MODE;
   const int tiles_y = (G.Y + TY - 1) / TY;
   const int x0 = (tile / tiles_y) * TX;
   const int y0 = (tile % tiles_y) * TY;
   StepState* st = A.st;
-  constexpr bool uses_v = mode == M_S2 || mode == M_S3 || mode == M_S4 || mode == M_S23;
+  constexpr bool uses_v = MODE == M_S2 || MODE == M_S3 || MODE == M_S23;
   // The arrest flag (set by the last block of stage 1) is read only after the TMA
   // copies are issued, so its global-memory round trip overlaps them.
   bool arrest = false;
@@ -658,11 +679,9 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
     if (!isnan(A.prev_energy)) st->E_last = A.prev_energy;
   }
 
-  // ---- stage the halo tile of T_s --------------------------------------
+  // ---- stage the halo tiles --------------------------------------------
   R* T = B0;
   if constexpr (TMA) {
-    constexpr bool need_v = uses_v;
-    const bool need_l = mode == M_S3 || mode == M_S4 || mode == M_S23;
     if (!issued) {
       if (threadIdx.x == 0) mbar_init(&bar, 1);
       __syncthreads();
@@ -675,17 +694,11 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
       mbar_wait_bounded(&bar, 0, A.wait_cycles);
       return;
     }
-    if constexpr (mode == M_S2 || mode == M_S23) {
-      if (A.copy_phi || A.copy_vel) {  // uniform over the block
-        copy_centre<NF, R, TX, TY, NT>(A, B0, B1, x0, y0);
-        __syncthreads();  // every value is copied before the combine overwrites V in place
-      }
-    }
-    if constexpr (mode == M_S23) {
+    using V = typename PairOf<R>::type;
+    const V half(0.5), hdt(grid_k<R>(G, GK_HDT));
+    if constexpr (MODE == M_S23) {
       // T3 = phi + dt/2 (V + l1/2) in place of l1 and T2 = phi + dt/2 V in place of V, in
       // one pass (each element reads its own phi, V, l1 before writing)
-      using V = typename PairOf<R>::type;
-      const V half(0.5), hdt(grid_k<R>(G, GK_HDT));
       for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
         V p0, p1, v0(0.0), v1(0.0), w0, w1;
         ld_quad(B0 + i, p0, p1);
@@ -695,102 +708,78 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
         st_quad(B1 + i, vfma(hdt, v0, p0), vfma(hdt, v1, p1));
       }
       __syncthreads();
-    } else if (mode == M_S2 || mode == M_S3 || mode == M_S4) {
-      // combine in place into the last staged buffer (OOB entries are zero in all)
-      R* dst = need_l ? B2 : (need_v ? B1 : B0);
-      if (dst != B0) {
-        using V = typename PairOf<R>::type;
-        const V half(0.5), hdt(grid_k<R>(G, GK_HDT)), dtv(grid_k<R>(G, GK_DT));
-        for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
-          V p0, p1, v0(0.0), v1(0.0), w0(0.0), w1(0.0);
-          ld_quad(B0 + i, p0, p1);
-          if (need_v && !arrest) ld_quad(B1 + i, v0, v1);
-          if (need_l) ld_quad(B2 + i, w0, w1);
-          V t0, t1;
-          if (mode == M_S2) {
-            t0 = vfma(hdt, v0, p0);
-            t1 = vfma(hdt, v1, p1);
-          } else if (mode == M_S3) {
-            t0 = vfma(hdt, vfma(half, w0, v0), p0);
-            t1 = vfma(hdt, vfma(half, w1, v1), p1);
-          } else {
-            t0 = vfma(dtv, vfma(half, w0, v0), p0);
-            t1 = vfma(dtv, vfma(half, w1, v1), p1);
-          }
-          st_quad(dst + i, t0, t1);
-        }
-        __syncthreads();
+    } else if constexpr (MODE == M_S2 || MODE == M_S3) {
+      // T2 in place of V, or T3 in place of l1 (OOB entries are zero in all)
+      R* dst = MODE == M_S3 ? B2 : B1;
+      for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
+        V p0, p1, v0(0.0), v1(0.0), w0(0.0), w1(0.0);
+        ld_quad(B0 + i, p0, p1);
+        if (!arrest) ld_quad(B1 + i, v0, v1);
+        if (MODE == M_S3) ld_quad(B2 + i, w0, w1);
+        if (MODE == M_S2)
+          st_quad(dst + i, vfma(hdt, v0, p0), vfma(hdt, v1, p1));
+        else
+          st_quad(dst + i, vfma(hdt, vfma(half, w0, v0), p0), vfma(hdt, vfma(half, w1, v1), p1));
       }
+      __syncthreads();
       T = dst;
     }
   } else {
     if constexpr (uses_v) arrest = st->arrest != 0;
-    stage_plain<NF, R, TX, TY, NT>(B0, A, x0, y0, mode, arrest);
-    if constexpr (mode == M_S2) {
-      if (A.copy_phi || A.copy_vel) copy_centre<NF, R, TX, TY, NT>(A, (const R*)nullptr, (const R*)nullptr, x0, y0);
-    }
+    stage_plain<NF, R, TX, TY, NT>(B0, A, x0, y0, MODE, arrest);
     __syncthreads();
   }
 
   double e_acc = 0.0;
   double err_max = -INFINITY;
-  const R* Praw = nullptr;
-  const R* Vraw = nullptr;
-  if constexpr (TMA) {
-    if (mode == M_S4) {
-      Praw = B0;
-      Vraw = arrest ? nullptr : B1;
-    }
-  }
   const bool fast = (G.Y % 2 == 0) && x0 >= G.halo + 1 && x0 + TX - 1 <= G.X - G.halo - 2 && y0 >= G.halo + 1 &&
                     y0 + TY - 1 <= G.Y - G.halo - 2;
-  // FP32 fields: the energy comes from the gradient stencil's jets; FP64 fields: from
-  // exact FP64 differences of the staged values (energy_tile)
-  constexpr bool JE = sizeof(R) == 4 && (MODE == M_S1 || MODE == M_ENERGY);
-  const bool je = JE && !(MODE == M_ENERGY && A.exact_energy);
   if constexpr (MODE == M_S23) {
-    // l3 from T3 (staged in B2), then l2 from T2 (staged in B1): the stage-3 and stage-2
-    // arithmetic per site, so the results equal the two separate stages bitwise
-    if (fast) {
-      grad_tile<TH, R, TX, TY, NT, true, M_S3>(A, B2, nullptr, nullptr, x0, y0, arrest, err_max, nullptr, nullptr,
-                                               nullptr, nullptr, A.out_l);
-      grad_tile<TH, R, TX, TY, NT, true, M_S2>(A, B1, nullptr, nullptr, x0, y0, arrest, err_max, nullptr, nullptr,
-                                               nullptr, nullptr, A.out_l2);
-    } else {
-      grad_tile<TH, R, TX, TY, NT, false, M_S3>(A, B2, nullptr, nullptr, x0, y0, arrest, err_max, nullptr, nullptr,
-                                                nullptr, nullptr, A.out_l);
-      grad_tile<TH, R, TX, TY, NT, false, M_S2>(A, B1, nullptr, nullptr, x0, y0, arrest, err_max, nullptr, nullptr,
-                                                nullptr, nullptr, A.out_l2);
-    }
+    // l3 from T3 (staged in B2) and l2 from T2 (staged in B1) per site pair, then the
+    // stage-4 inputs: the stage-2 and stage-3 arithmetic, so the results equal the two
+    // separate stages bitwise
+    if (fast)
+      grad_tile<TH, R, TX, TY, NT, true, M_S23>(A, B2, x0, y0, arrest, err_max, nullptr, B0, nullptr, B1);
+    else
+      grad_tile<TH, R, TX, TY, NT, false, M_S23>(A, B2, x0, y0, arrest, err_max, nullptr, B0, nullptr, B1);
     return;
-  }
-  if constexpr (MODE != M_ENERGY || JE) {
-    if (MODE != M_ENERGY || je) {
-      double* ep = (je && do_energy) ? &e_acc : nullptr;
+  } else if constexpr (MODE == M_S1 || MODE == M_ENERGY) {
+    // FP32 fields: the flow energy from the stencil's jets (stage 1 and the trailing
+    // pass), or (observables) the exact FP64 differences of the stored values; FP64
+    // fields: the exact differences
+    constexpr bool JE = sizeof(R) == 4;
+    const bool je = JE && !(MODE == M_ENERGY && A.exact_energy);
+    double* ep = (je && do_energy) ? &e_acc : nullptr;
+    if (MODE == M_S1 || je) {
       if (fast)
-        grad_tile<TH, R, TX, TY, NT, true, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, nullptr, nullptr, ep);
+        grad_tile<TH, R, TX, TY, NT, true, MODE, JE>(A, T, x0, y0, false, err_max, ep);
       else
-        grad_tile<TH, R, TX, TY, NT, false, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, nullptr, nullptr,
-                                                     ep);
+        grad_tile<TH, R, TX, TY, NT, false, MODE, JE>(A, T, x0, y0, false, err_max, ep);
     }
-  }
-  if constexpr (MODE == M_S1 || MODE == M_ENERGY) {
     if (do_energy && !je) {
       if (fast)
         e_acc = energy_tile<TH, R, TX, TY, NT, true>(A, T, x0, y0);
       else
         e_acc = energy_tile<TH, R, TX, TY, NT, false>(A, T, x0, y0);
     }
+  } else {
+    // S2, S3, S4, M_GRAD; stage 3 combines with the staged phi and V (TMA staging)
+    const R* Praw = (TMA && MODE == M_S3) ? B0 : nullptr;
+    const R* Vraw = (TMA && MODE == M_S3) ? B1 : nullptr;
+    if (fast)
+      grad_tile<TH, R, TX, TY, NT, true, MODE>(A, T, x0, y0, arrest, err_max, nullptr, Praw, Vraw);
+    else
+      grad_tile<TH, R, TX, TY, NT, false, MODE>(A, T, x0, y0, arrest, err_max, nullptr, Praw, Vraw);
   }
 
   // ---- reductions -------------------------------------------------------
-  const bool need_ticket = do_energy || mode == M_S4;
+  const bool need_ticket = do_energy || MODE == M_S4;
   if (!need_ticket) return;
   if (do_energy) {
     const double bs = block_sum_fixed<NT>(e_acc, red);
     if (threadIdx.x == 0) A.partial[tile] = bs;
   }
-  if (mode == M_S4) {
+  if (MODE == M_S4) {
     const double bm = block_max<NT>(err_max, red);
     if (threadIdx.x == 0 && bm > -INFINITY) atomicMax(&st->err_enc, enc_max(bm));
   }
@@ -815,7 +804,7 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
     }
   }
   if (threadIdx.x == 0) {
-    if (mode == M_S4) {
+    if (MODE == M_S4) {
       const double err = dec_max(atomicExch(&st->err_enc, 0ULL));
       if (A.err_traj && A.err_idx >= 0) A.err_traj[A.err_idx] = err;
     }
@@ -823,8 +812,17 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   }
 }
 
+// Resident CTAs per SM a one-tile-per-CTA stage kernel is built for: three 256-thread
+// CTAs (80 registers) for the fused FP32 stages 2+3, whose two stencils per site pair
+// would otherwise take the registers of one of them (staging latency is hidden only by
+// other resident CTAs); no bound otherwise.
+template <typename R, int MODE, int NT>
+__host__ __device__ constexpr int flow_min_ctas() {
+  return (sizeof(R) == 4 && MODE == M_S23 && NT == 256) ? 3 : 1;
+}
+
 template <class TH, typename R, int TX, int TY, int NT, bool TMA, int MODE>
-__global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowArgs<R> A) {
+__global__ void __launch_bounds__(NT, (flow_min_ctas<R, MODE, NT>())) flow_kernel(const __grid_constant__ FlowArgs<R> A) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ StageShared<NT> S;
   flow_tile<TH, R, TX, TY, NT, TMA, MODE>(A, &A.tm_phi, &A.tm_vel, &A.tm_l, blockIdx.x, gridDim.x, smem_raw, S);
@@ -834,12 +832,12 @@ __global__ void __launch_bounds__(NT) flow_kernel(const __grid_constant__ FlowAr
 // Persistent, TMA-pipelined form of flow_kernel (FP32 fields): one CTA per SM
 // walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ... through a ring of STAGES
 // shared-memory slots, so the bulk tensor loads of the next tiles are in flight
-// while the current tile is computed.  Stage 4 also stages the centre tiles of l1
-// and l3.  Energy partials are per CTA in tile order (deterministic for a fixed grid).
+// while the current tile is computed.  Stage 4 also stages the centre tiles of cP and cV.
+// Energy partials are per CTA in tile order (deterministic for a fixed grid).
 // ---------------------------------------------------------------------------
 template <int MODE>
 __host__ __device__ constexpr int pipe_halo_buffers() {
-  return MODE == M_S2 ? 2 : (MODE == M_S3 || MODE == M_S4) ? 3 : 1;
+  return flow_buffers(MODE);
 }
 template <int MODE>
 __host__ __device__ constexpr int pipe_centre_buffers() {
@@ -854,8 +852,7 @@ __host__ __device__ constexpr size_t pipe_slot_bytes() {
 // Persistent CTAs per SM: for stage 1 and the energy pass the theory's S1_CTAS (four
 // 256-thread CTAs for the light chiral stencil, issue-bound: two site pairs per thread
 // per tile halve the per-tile overhead, and four CTAs keep 32 warps per SM), one
-// 512-thread CTA otherwise.  Stage 1 and the energy pass must agree: their partials
-// are per CTA.
+// 512-thread CTA otherwise.
 template <class TH, int MODE>
 __host__ __device__ constexpr int pipe_ctas() {
   return (MODE == M_S1 || MODE == M_ENERGY) ? TH::S1_CTAS : 1;
@@ -872,6 +869,7 @@ __global__ void __launch_bounds__(NT, (pipe_ctas<TH, MODE>())) flow_kernel_pipe(
   constexpr int BUF = NF * TS::PLANE;             // elements of one halo buffer
   constexpr int CBUF = NF * TX * TY;              // elements of one centre buffer
   constexpr int SLOT = BUF * pipe_halo_buffers<MODE>() + CBUF * pipe_centre_buffers<MODE>();
+  static_assert(MODE != M_S23, "the fused stages 2+3 run one tile per CTA");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   R* ring = reinterpret_cast<R*>(smem_raw);
   __shared__ double red[NT / 32];
@@ -884,11 +882,12 @@ __global__ void __launch_bounds__(NT, (pipe_ctas<TH, MODE>())) flow_kernel_pipe(
   const int tiles_y = (G.Y + TY - 1) / TY;
   const int ntiles = ((G.X + TX - 1) / TX) * tiles_y;
   StepState* st = A.st;
-  const bool arrest = (MODE == M_S2 || MODE == M_S3 || MODE == M_S4) && (st->arrest != 0);
+  const bool arrest = (MODE == M_S2 || MODE == M_S3) && (st->arrest != 0);
   const bool do_energy = (MODE == M_S1 || MODE == M_ENERGY) && A.with_energy != 0;
-  const bool need_v = (MODE == M_S2 || MODE == M_S3 || MODE == M_S4) && !arrest;
-  constexpr bool need_l = MODE == M_S3 || MODE == M_S4;
-  const uint32_t bytes = (uint32_t)(sizeof(R) * (BUF * (1 + (need_v ? 1 : 0) + (need_l ? 1 : 0)) +
+  // second halo buffer: V in S2 / S3 (not loaded when arrested)
+  const bool load_b1 = (MODE == M_S2 || MODE == M_S3) && !arrest;
+  constexpr bool load_b2 = MODE == M_S3;
+  const uint32_t bytes = (uint32_t)(sizeof(R) * (BUF * (1 + (load_b1 ? 1 : 0) + (load_b2 ? 1 : 0)) +
                                                  CBUF * pipe_centre_buffers<MODE>()));
 
   if (A.init_state && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -900,11 +899,11 @@ __global__ void __launch_bounds__(NT, (pipe_ctas<TH, MODE>())) flow_kernel_pipe(
     const int x0 = (tile / tiles_y) * TX, y0 = (tile % tiles_y) * TY;
     mbar_expect_tx(&full[slot], bytes + A.tx_extra);
     tma_load_3d(base, &A.tm_phi, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
-    if (need_v) tma_load_3d(base + BUF, &A.tm_vel, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
-    if (need_l) tma_load_3d(base + 2 * BUF, &A.tm_l, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
+    if (load_b1) tma_load_3d(base + BUF, &A.tm_vel, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
+    if (load_b2) tma_load_3d(base + 2 * BUF, &A.tm_l, y0 - TS::YOFF, x0 - 2, 0, &full[slot]);
     if (MODE == M_S4) {
-      tma_load_3d(base + 3 * BUF, &A.tm_c1, y0, x0, 0, &full[slot]);
-      tma_load_3d(base + 3 * BUF + CBUF, &A.tm_c3, y0, x0, 0, &full[slot]);
+      tma_load_3d(base + BUF, &A.tm_cp, y0, x0, 0, &full[slot]);
+      tma_load_3d(base + BUF + CBUF, &A.tm_cv, y0, x0, 0, &full[slot]);
     }
   };
   if (threadIdx.x == 0) {
@@ -951,74 +950,63 @@ __global__ void __launch_bounds__(NT, (pipe_ctas<TH, MODE>())) flow_kernel_pipe(
       ++tx;
     }
     R* T = B0;
-    // Stage 4 combines T4 into the staged l2 tile in place, but the finalize needs l2
-    // at the thread's own sites: keep that pair in registers (one pass per thread)
-    // instead of re-reading it from global memory.
-    using VP = typename PairOf<R>::type;
-    constexpr bool L2REG = MODE == M_S4 && TX * (TY / 2) == NT;
-    VP l2c[L2REG ? NF : 1];
-    if constexpr (L2REG) {
-      const int toff = (threadIdx.x / (TY / 2) + 2) * TS::HY + TS::YOFF + 2 * (threadIdx.x % (TY / 2));
-#pragma unroll
-      for (int a = 0; a < NF; ++a) l2c[a] = ld_pair(B2 + a * TS::PLANE + toff);
-      __syncthreads();  // every pair is read before the combine overwrites the tile
-    }
-    if (MODE == M_S2 || MODE == M_S3 || MODE == M_S4) {
-      R* dst = need_l ? B2 : (need_v ? B1 : B0);
-      if (dst != B0) {
-        using V = typename PairOf<R>::type;
-        const V half(0.5), hdt(grid_k<R>(G, GK_HDT)), dtv(grid_k<R>(G, GK_DT));
-        for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
-          V p0, p1, v0(0.0), v1(0.0), w0(0.0), w1(0.0);
-          ld_quad(B0 + i, p0, p1);
-          if (need_v) ld_quad(B1 + i, v0, v1);
-          if (need_l) ld_quad(B2 + i, w0, w1);
-          V t0, t1;
-          if (MODE == M_S2) {
-            t0 = vfma(hdt, v0, p0);
-            t1 = vfma(hdt, v1, p1);
-          } else if (MODE == M_S3) {
-            t0 = vfma(hdt, vfma(half, w0, v0), p0);
-            t1 = vfma(hdt, vfma(half, w1, v1), p1);
-          } else {
-            t0 = vfma(dtv, vfma(half, w0, v0), p0);
-            t1 = vfma(dtv, vfma(half, w1, v1), p1);
-          }
-          st_quad(dst + i, t0, t1);
-        }
-        __syncthreads();
+    if constexpr (MODE == M_S2 || MODE == M_S3) {
+      // T2 in place of V, or T3 in place of l1
+      R* dst = MODE == M_S3 ? B2 : B1;
+      using V = typename PairOf<R>::type;
+      const V half(0.5), hdt(grid_k<R>(G, GK_HDT));
+      for (int i = 4 * threadIdx.x; i < BUF; i += 4 * NT) {
+        V p0, p1, v0(0.0), v1(0.0), w0(0.0), w1(0.0);
+        ld_quad(B0 + i, p0, p1);
+        if (!arrest) ld_quad(B1 + i, v0, v1);
+        if (MODE == M_S3) ld_quad(B2 + i, w0, w1);
+        if (MODE == M_S2)
+          st_quad(dst + i, vfma(hdt, v0, p0), vfma(hdt, v1, p1));
+        else
+          st_quad(dst + i, vfma(hdt, vfma(half, w0, v0), p0), vfma(hdt, vfma(half, w1, v1), p1));
       }
+      __syncthreads();
       T = dst;
     }
-    const R* Praw = MODE == M_S4 ? B0 : nullptr;
-    const R* Vraw = (MODE == M_S4 && !arrest) ? B1 : nullptr;
-    const R* C1 = MODE == M_S4 ? base + 3 * BUF : nullptr;
-    const R* C3 = MODE == M_S4 ? base + 3 * BUF + CBUF : nullptr;
     const bool fast = (G.Y % 2 == 0) && x0 >= G.halo + 1 && x0 + TX - 1 <= G.X - G.halo - 2 &&
                       y0 >= G.halo + 1 && y0 + TY - 1 <= G.Y - G.halo - 2;
-    constexpr bool JE = sizeof(R) == 4 && (MODE == M_S1 || MODE == M_ENERGY);
-    // the four-CTA energy pass is built for the flow energy only (the exact FP64 energy
-    // would spill out of its 64 registers); the host sends exact energies to flow_kernel
-    constexpr bool EXACT = !(MODE == M_ENERGY && pipe_ctas<TH, MODE>() == 4);
-    const bool je = JE && !(MODE == M_ENERGY && EXACT && A.exact_energy);
-    if constexpr (MODE != M_ENERGY || JE) {
-      if (MODE != M_ENERGY || je) {
-        double* ep = (je && do_energy) ? &e_acc : nullptr;
+    if constexpr (MODE == M_S4) {
+      const R* Cp = base + BUF;
+      const R* Cv = base + BUF + CBUF;
+      if (fast)
+        grad_tile<TH, R, TX, TY, NT, true, M_S4>(A, T, x0, y0, false, err_max, nullptr, nullptr, nullptr, nullptr, Cp,
+                                                 Cv);
+      else
+        grad_tile<TH, R, TX, TY, NT, false, M_S4>(A, T, x0, y0, false, err_max, nullptr, nullptr, nullptr, nullptr, Cp,
+                                                  Cv);
+    } else if constexpr (MODE == M_S1 || MODE == M_ENERGY) {
+      constexpr bool JE = sizeof(R) == 4;
+      // the four-CTA energy pass is built for the flow energy only (the exact FP64 energy
+      // would spill out of its 64 registers); the host sends exact energies to flow_kernel
+      constexpr bool EXACT = !(MODE == M_ENERGY && pipe_ctas<TH, MODE>() == 4);
+      const bool je = JE && !(MODE == M_ENERGY && EXACT && A.exact_energy);
+      double* ep = (je && do_energy) ? &e_acc : nullptr;
+      if (MODE == M_S1 || je) {
         if (fast)
-          grad_tile<TH, R, TX, TY, NT, true, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3, ep,
-                                                      L2REG ? l2c : nullptr);
+          grad_tile<TH, R, TX, TY, NT, true, MODE, JE>(A, T, x0, y0, false, err_max, ep);
         else
-          grad_tile<TH, R, TX, TY, NT, false, MODE, JE>(A, T, Praw, Vraw, x0, y0, arrest, err_max, C1, C3, ep,
-                                                       L2REG ? l2c : nullptr);
+          grad_tile<TH, R, TX, TY, NT, false, MODE, JE>(A, T, x0, y0, false, err_max, ep);
       }
-    }
-    if constexpr ((MODE == M_S1 || MODE == M_ENERGY) && EXACT) {
-      if (do_energy && !je) {
-        if (fast)
-          e_acc += energy_tile<TH, R, TX, TY, NT, true>(A, T, x0, y0);
-        else
-          e_acc += energy_tile<TH, R, TX, TY, NT, false>(A, T, x0, y0);
+      if constexpr (EXACT) {
+        if (do_energy && !je) {
+          if (fast)
+            e_acc += energy_tile<TH, R, TX, TY, NT, true>(A, T, x0, y0);
+          else
+            e_acc += energy_tile<TH, R, TX, TY, NT, false>(A, T, x0, y0);
+        }
       }
+    } else {
+      const R* Praw = MODE == M_S3 ? B0 : nullptr;
+      const R* Vraw = MODE == M_S3 ? B1 : nullptr;
+      if (fast)
+        grad_tile<TH, R, TX, TY, NT, true, MODE>(A, T, x0, y0, arrest, err_max, nullptr, Praw, Vraw);
+      else
+        grad_tile<TH, R, TX, TY, NT, false, MODE>(A, T, x0, y0, arrest, err_max, nullptr, Praw, Vraw);
     }
     __syncthreads();  // every thread is done with this slot
     if (threadIdx.x == 0) {
@@ -1067,18 +1055,12 @@ __global__ void __launch_bounds__(NT, (pipe_ctas<TH, MODE>())) flow_kernel_pipe(
   }
 }
 
-// Apply a pending arrest (V = 0) left by the trailing energy pass, and copy the result
-// back into the caller's buffers when `copy` says it sits in the alternates (the fused
-// step never leaves it there: the last step of an odd count writes the caller's buffers).
+// Apply a pending arrest (V = 0) left by the trailing energy pass at the end of a call.
 template <typename R>
-__global__ void finish_kernel(const R* __restrict__ phi_src, const R* __restrict__ vel_src, R* phi_dst,
-                              R* vel_dst, long long n, int copy, const StepState* st) {
-  const bool arrest = st->arrest != 0;
-  if (!copy && !arrest) return;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    if (copy) phi_dst[i] = phi_src[i];
-    if (copy || arrest) vel_dst[i] = arrest ? (R)0 : vel_src[i];
-  }
+__global__ void finish_kernel(R* vel, long long n, const StepState* st) {
+  if (st->arrest == 0) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    vel[i] = (R)0;
 }
 
 // ---------------------------------------------------------------------------

@@ -63,7 +63,7 @@ def test_create_and_workspace_size():
     assert rc == 0
     n = ctypes.c_size_t()
     assert lib.ss_workspace_bytes(h, ctypes.byref(n)) == 0
-    # l1..l3 and the ping-pong Field/Velocity copies: 5 FP32 field-sized buffers at least
+    # l1, l2, T4 and stage 4's two accumulated inputs: 5 FP32 field-sized buffers at least
     assert n.value >= 5 * 4 * 4 * 100 * 70
     assert lib.ss_destroy(h) == 0
 

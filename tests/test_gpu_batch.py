@@ -70,9 +70,9 @@ def test_batch_matches_single_lattices(precision, aligned):
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 @pytest.mark.parametrize("aligned", [True, False], ids=["tma", "plain"])
 def test_batch_odd_step_counts_are_bitwise_invariant(aligned, precision):
-    """The last step of an odd-count batched call ends in the caller's buffers (stage 2
-    copies phi and V into the alternates, stage 4 runs at the opposite parity): seven
-    steps split into odd and even calls equal one call bitwise, arrests included."""
+    """Batched steps update every lattice's buffers in place (stage 4 reads only T4, cV
+    and cP): seven steps split into odd and even calls equal one call bitwise, arrests
+    included."""
     th = load_theory("Baby Skyrme")
     sizes = [s for s in SIZES if (s[1] % 4 == 0) == aligned]
     rng = np.random.default_rng(11)

@@ -234,8 +234,8 @@ def test_projected_energy_vs_oracle(th, kw, prec):
 
 
 def test_step_chunking_is_bitwise_invariant():
-    """Ten steps in one call equal 3 + 7 steps: the fused energy of the next stage 1
-    and the trailing energy pass use the same tiles and the same reduction order."""
+    """Ten steps in one call equal 3 + 7 and 1 + 1 + 8 steps: every step updates the
+    caller's buffers in place and reduces its energy in stage 4, whatever the split."""
     theory = load_theory("Chiral magnet")
     rp = theory.params.default_params(xlen=150, ylen=140, xsize=10.0, ysize=10.0, dmi_term="Heusler", demag=True,
                                       unit_magnetization=True).resolved()
@@ -286,11 +286,12 @@ def test_step_across_trajectory_chunks_equals_one_async_call():
 
 @pytest.mark.parametrize("Y", [192, 150], ids=["tma", "plain"])
 def test_odd_step_counts_every_variant(Y):
-    """A call with an odd step count ends in the caller's buffers without a copy back:
-    stage 2 (one tile per CTA, fused with stage 3 or not, TMA-staged or plain) copies
-    phi and V into the alternates and stage 4 writes the caller's buffers; a pipelined
-    stage 2 copies with plain memcpys.  Splits of seven steps into odd and even calls
-    agree bitwise with one call, under every variant pinning, with arrests on."""
+    """Every staging variant computes the same per-site arithmetic: stage 4 reads only
+    T4, cV and cP (written by stage 3, fused with stage 2 or not, TMA-staged or plain)
+    and updates the caller's buffers in place.  Splits of seven steps into odd and even
+    calls agree bitwise with one call, under every variant pinning (pipelined or one
+    tile per CTA), with arrests on; energies agree to rounding (per-CTA or per-tile
+    partials)."""
     theory = load_theory("Chiral magnet")
     rp = theory.params.default_params(xlen=256, ylen=Y, xsize=10.0, ysize=7.5, dmi_term="Heusler", demag=True,
                                       unit_magnetization=True, killkinen=True).resolved()
@@ -332,11 +333,12 @@ FLOW_E = [("chiral_magnet", dict(xlen=150, ylen=140, xsize=10.0, ysize=10.0, dmi
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])
 @pytest.mark.parametrize("th,kw", FLOW_E, ids=[t for t, _ in FLOW_E])
 def test_flow_energy_vs_observable(th, kw, prec):
-    """The flow's per-step energy (stage 1 and the trailing pass) against the energy
-    observable of the same field.  FP64 fields: one code path, bitwise equal.  FP32
-    fields: the flow evaluates the energy point on the gradient stencil's FP32 jets
-    (packed FP32 for the chiral magnet, FP64 on converted jets otherwise) while the
-    observable is the FP64 stencil of the stored values; both reduce in FP64."""
+    """The flow's per-step energy (reduced by stage 4 from its re-projected cP tile,
+    the values it stores as phi') against the energy observable of the same field.
+    FP64 fields: the same exact stencil over the same tiles, bitwise equal.  FP32
+    fields: the flow evaluates the energy point on FP32 jets (packed FP32 for the
+    chiral magnet, FP64 on converted jets otherwise) while the observable is the FP64
+    stencil of the stored values; both reduce in FP64."""
     theory = load_theory(NAMES[th])
     rp = theory.params.default_params(**kw).resolved()
     p_i, p_f = theory.params.pack_device_params(rp)
