@@ -588,15 +588,14 @@ struct Fused {
         if ((rc = launch(h, A, true))) break;
       }
       set_mode(m);
-      if (!uses_pipe(m)) {
-        h->use_pipe[m] = 0;
-        continue;
-      }
-      for (int v = 0; v < 2 && rc == SS_OK; ++v) {
+      // the one-tile-per-CTA variant always (its time enters the fusion decision below),
+      // the pipelined one where it exists
+      const bool pipe = uses_pipe(m);
+      for (int v = 0; v < (pipe ? 2 : 1) && rc == SS_OK; ++v) {
         h->use_pipe[m] = v;
         rc = time_mode(h->tune_ms[m][v]);
       }
-      h->use_pipe[m] = h->tune_ms[m][1] <= h->tune_ms[m][0] ? 1 : 0;
+      h->use_pipe[m] = (pipe && h->tune_ms[m][1] <= h->tune_ms[m][0]) ? 1 : 0;
     }
     // the energy-only pass must reduce exactly like stage 1 (same grid and tile order)
     h->use_pipe[M_ENERGY] = h->use_pipe[M_S1];

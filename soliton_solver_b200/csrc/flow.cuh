@@ -433,6 +433,19 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, int 
     }
     const int toff = (lx + 2) * TS::HY + TS::YOFF + 2 * j;
     const long long sidx = (long long)gx * G.Y + gy;
+    // M_S23: the pair's V and l1 (overwritten by T2 and T3 in shared memory) come back
+    // from L2; issued before the two stencils so that their latency hides behind them
+    // (up to four components: the six of the s+id model would spill)
+    constexpr bool PRE = MODE == M_S23 && NF <= 4;
+    constexpr int NPRE = PRE ? NF : 1;
+    V pre_v[NPRE], pre_l1[NPRE];
+    if constexpr (PRE) {
+#pragma unroll
+      for (int a = 0; a < NF; ++a) {
+        pre_v[a] = arrest ? V(0.0) : gload<V, R>(A.vel + a * N + sidx, FAST, v1);
+        pre_l1[a] = gload<V, R>(A.la + a * N + sidx, FAST, v1);
+      }
+    }
 
     Jet<V, NF> J;
     tile_jet<TH, V, R, TS::HY, TS::PLANE, FAST>(T, toff, kc, m0, m1, J);
@@ -512,8 +525,14 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, int 
       for (int a = 0; a < NF; ++a) {
         const long long idx = a * N + sidx;
         const V p = Praw ? ld_pair(Praw + a * TS::PLANE + toff) : gload<V, R>(A.phi + idx, FAST, v1);
-        const V v = arrest ? V(0.0) : (Vraw ? ld_pair(Vraw + a * TS::PLANE + toff) : gload<V, R>(A.vel + idx, FAST, v1));
-        const V l1 = gload<V, R>(A.la + idx, FAST, v1);
+        V v, l1;
+        if constexpr (PRE) {
+          v = pre_v[a];
+          l1 = pre_l1[a];
+        } else {
+          v = arrest ? V(0.0) : (Vraw ? ld_pair(Vraw + a * TS::PLANE + toff) : gload<V, R>(A.vel + idx, FAST, v1));
+          l1 = gload<V, R>(A.la + idx, FAST, v1);
+        }
         const V l3 = mdt * g[a];
         gstore<V, R>(A.out_t4 + idx, vfma(dtv, vfma(half, l2[a], v), p), FAST, v1);
         gstore<V, R>(A.out_cv + idx, vfma(sixth, vfma(two, l3, vfma(two, l2[a], l1)), v), FAST, v1);
@@ -812,17 +831,24 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
   }
 }
 
-// Resident CTAs per SM a one-tile-per-CTA stage kernel is built for: three 256-thread
-// CTAs (80 registers) for the fused FP32 stages 2+3, whose two stencils per site pair
-// would otherwise take the registers of one of them (staging latency is hidden only by
-// other resident CTAs); no bound otherwise.
-template <typename R, int MODE, int NT>
+// Resident CTAs per SM a one-tile-per-CTA stage kernel is built for (the staging latency
+// of a tile is hidden only by other resident CTAs).  The fused FP32 stages 2+3 evaluate
+// two stencils per site pair: capped at three 256-thread CTAs (80 registers) for the
+// theories with up to four components and at two (128 registers; its 104 KB of staging
+// fits two anyway) for the six-component s+id.  FP64 stage 4 (one staged buffer) at two
+// 256-thread CTAs, 128 registers, up to four components (the s+id would spill ~380
+// bytes).  No bound otherwise.
+template <class TH, typename R, int MODE, int NT>
 __host__ __device__ constexpr int flow_min_ctas() {
-  return (sizeof(R) == 4 && MODE == M_S23 && NT == 256) ? 3 : 1;
+  if (NT != 256) return 1;
+  if (sizeof(R) == 4 && MODE == M_S23) return TH::NF <= 4 ? 3 : 2;
+  if (sizeof(R) == 8 && MODE == M_S4) return TH::NF <= 4 ? 2 : 1;
+  return 1;
 }
 
 template <class TH, typename R, int TX, int TY, int NT, bool TMA, int MODE>
-__global__ void __launch_bounds__(NT, (flow_min_ctas<R, MODE, NT>())) flow_kernel(const __grid_constant__ FlowArgs<R> A) {
+__global__ void __launch_bounds__(NT, (flow_min_ctas<TH, R, MODE, NT>()))
+    flow_kernel(const __grid_constant__ FlowArgs<R> A) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ StageShared<NT> S;
   flow_tile<TH, R, TX, TY, NT, TMA, MODE>(A, &A.tm_phi, &A.tm_vel, &A.tm_l, blockIdx.x, gridDim.x, smem_raw, S);
