@@ -69,22 +69,69 @@ def config(extra=None):
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class Clocks:
-    """nvidia-smi sampler (20 ms period); summary() keeps the samples between the
-    first and last mark() (the timed region)."""
+    """SM clock, power and clock-event reasons of this rank's GPU, sampled while the
+    benchmark runs; summary() keeps the samples between the first and last mark() (the
+    timed region).  NVML is polled every millisecond from a thread (the timed region of a
+    short run lasts ~15 ms); without NVML, nvidia-smi samples every 20 ms.  Raw samples go
+    to SS_BENCH_CLOCKS_DIR when set."""
 
     Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.thread = None
+        self.samples = []  # (time, sm MHz, max sm MHz, power W, set of reasons)
         self.marks = []
-        # raw samples: SS_BENCH_CLOCKS_DIR when set (to keep them), else the temp directory
         out = os.environ.get("SS_BENCH_CLOCKS_DIR") or tempfile.gettempdir()
         self.path = os.path.join(out, f"clocks_gpu{index}.csv")
 
+    def _nvml_handle(self, nv):
+        """NVML handle of the CUDA device `index` (matched by UUID: CUDA_VISIBLE_DEVICES
+        may renumber), else NVML's device `index`."""
+        try:
+            import torch
+            want = str(torch.cuda.get_device_properties(self.index).uuid).lower()
+            for i in range(nv.nvmlDeviceGetCount()):
+                h = nv.nvmlDeviceGetHandleByIndex(i)
+                u = nv.nvmlDeviceGetUUID(h)
+                u = (u.decode() if isinstance(u, bytes) else u).lower()
+                if want and want in u:
+                    return h
+        except Exception:
+            pass
+        return nv.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll(self, nv, h, stop):
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not stop.is_set():
+            try:
+                t = time.time()
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((t, sm, smax, pw, {n for n, b in zip(self.NAMES, bits) if rs & b}))
+            except Exception:
+                break
+            stop.wait(0.001)
+
     def __enter__(self):
+        import threading
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            self._stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(nv, h, self._stop), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
@@ -100,6 +147,14 @@ class Clocks:
         self.marks.append(time.time())
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self._stop.set()
+            self.thread.join(timeout=5)
+            if os.environ.get("SS_BENCH_CLOCKS_DIR"):
+                os.makedirs(os.path.dirname(self.path), exist_ok=True)
+                with open(self.path, "w") as fh:
+                    for t, sm, smax, pw, rs in self.samples:
+                        fh.write(f"{t:.6f},{sm:.0f},{smax:.0f},{pw:.1f},{'|'.join(sorted(rs))}\n")
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -108,31 +163,35 @@ class Clocks:
                 self.proc.kill()
             self.fh.close()
 
-    def summary(self):
+    def _smi_samples(self):
         import datetime
-        if self.proc is None or not os.path.exists(self.path):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        lo, hi = (self.marks[0], self.marks[-1]) if len(self.marks) >= 2 else (-math.inf, math.inf)
-        sm, smax, power, reasons = [], [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        out = []
         for line in open(self.path).read().strip().splitlines():
             r = [x.strip() for x in line.split(",")]
             if len(r) < 10:
                 continue
             try:
                 t = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
-                if not (lo <= t <= hi):
-                    continue
-                sm.append(float(r[2]))
-                smax.append(float(r[3]))
-                power.append(float(r[4]))
+                out.append((t, float(r[2]), float(r[3]), float(r[4]),
+                            {n for n, v in zip(self.NAMES, r[6:10]) if v.lower() == "active"}))
             except ValueError:
                 continue
-            for n, v in zip(names, r[6:10]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "power_w_max": max(power) if power else None, "reasons": sorted(reasons), "samples": len(sm)}
+        return out
+
+    def summary(self):
+        if self.thread is not None:
+            samples, source = self.samples, "nvml, 1 ms"
+        elif self.proc is not None and os.path.exists(self.path):
+            samples, source = self._smi_samples(), "nvidia-smi, 20 ms"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        lo, hi = (self.marks[0], self.marks[-1]) if len(self.marks) >= 2 else (-math.inf, math.inf)
+        sel = [x for x in samples if lo <= x[0] <= hi]
+        reasons = set().union(*[x[4] for x in sel]) if sel else set()
+        return {"sm_mhz": float(np.median([x[1] for x in sel])) if sel else None,
+                "sm_max_mhz": max(x[2] for x in sel) if sel else None,
+                "power_w_max": max(x[3] for x in sel) if sel else None, "reasons": sorted(reasons),
+                "samples": len(sel), "source": source}
 
 
 # ---------------------------------------------------------------------------
