@@ -133,9 +133,11 @@ struct ss_handle {
   mutable int inject_timeout = 0;  // test hook, consumed by the next flow launch
   cudaGraphExec_t graph = nullptr;  // captured n-step relaxation (ss_graph_create)
   const double* force = nullptr;    // FP64 flows: field added to the gradient rows (ss_set_forcing)
-  // page-locked host staging of ss_step: energy and err trajectories of one chunk and
-  // the StepState, copied with one synchronisation (allocated on the first ss_step)
+  // mapped page-locked staging of ss_step, written by the kernels themselves: the energy
+  // and err trajectories of one chunk and the status of the call (allocated on the first
+  // ss_step; host_stage_dev is its device address)
   double* host_stage = nullptr;
+  double* host_stage_dev = nullptr;
   ~ss_handle() {
     if (graph) cudaGraphExecDestroy(graph);
     if (host_stage) cudaFreeHost(host_stage);
@@ -453,7 +455,8 @@ struct Fused {
   }
 
   // n flow steps of the bound buffers, in place; trajectories to device arrays (nullable)
-  static int step(ss_handle* h, int n, double prev, double* E_dev, double* err_dev) {
+  // status_out (nullable, device-visible): the finish kernel copies the call's status there
+  static int step(ss_handle* h, int n, double prev, double* E_dev, double* err_dev, int* status_out = nullptr) {
     if (n <= 0) return SS_OK;
     R* field = (R*)h->field;
     R* vel = (R*)h->vel;
@@ -531,7 +534,7 @@ struct Fused {
     int rc = launch(h, A, tma);
     if (rc) return rc;
     const long long nfN = (long long)h->nf * h->G.N;
-    finish_kernel<R><<<grid_1d(nfN), 256, 0, h->stream>>>(vel, nfN, h->st);
+    finish_kernel<R><<<grid_1d(nfN), 256, 0, h->stream>>>(vel, nfN, h->st, status_out);
     CK(cudaGetLastError());
     return SS_OK;
   }
@@ -906,6 +909,7 @@ int ss_workspace_bytes(const ss_handle* h, size_t* bytes) {
   ss_handle tmp = *h;
   tmp.graph = nullptr;  // the copy must not own the original's graph or staging
   tmp.host_stage = nullptr;
+  tmp.host_stage_dev = nullptr;
   *bytes = layout(&tmp, nullptr);
   return SS_OK;
 }
@@ -1030,27 +1034,35 @@ int ss_step(ss_handle* h, int n_steps, double prev_energy, double* energy_traj, 
     });
   }
   if (n_steps == 0) return take_status(h);
-  // each chunk's trajectories and the device state come back through page-locked
-  // staging: the copies queue behind the kernels and one synchronisation waits for all
-  if (!h->host_stage)
-    CK(cudaHostAlloc((void**)&h->host_stage, 2 * TRAJ_CAP * sizeof(double) + sizeof(StepState),
-                     cudaHostAllocDefault));
+  // each chunk's trajectories and status are written by the kernels into mapped
+  // page-locked memory: one synchronisation per chunk and no copies
+  if (!h->host_stage) {
+    CK(cudaHostAlloc((void**)&h->host_stage, 2 * TRAJ_CAP * sizeof(double) + 64, cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer((void**)&h->host_stage_dev, h->host_stage, 0));
+  }
   double* hE = h->host_stage;
   double* hErr = h->host_stage + TRAJ_CAP;
-  StepState* hs = reinterpret_cast<StepState*>(h->host_stage + 2 * TRAJ_CAP);
+  volatile int* hstatus = reinterpret_cast<volatile int*>(h->host_stage + 2 * TRAJ_CAP);
+  int* dstatus = reinterpret_cast<int*>(h->host_stage_dev + 2 * TRAJ_CAP);
   double prev = prev_energy;
   for (int done = 0; done < n_steps; done += TRAJ_CAP) {
     const int k = std::min(TRAJ_CAP, n_steps - done);
-    rc = ss_step_async(h, k, prev, h->traj_E, h->traj_err);
+    *hstatus = -1;
+    rc = dispatch(h, [&](auto* tag) -> int {
+      using TH = std::remove_pointer_t<decltype(tag)>;
+      double* dE = h->host_stage_dev;
+      double* dErr = h->host_stage_dev + TRAJ_CAP;
+      if (h->precision == SS_FP32) return Fused<TH, float>::step(h, k, prev, dE, dErr, dstatus);
+      return Fused<TH, double>::step(h, k, prev, dE, dErr, dstatus);
+    });
     if (rc) return rc;
     prev = NAN;
-    if (energy_traj) CK(cudaMemcpyAsync(hE, h->traj_E, k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    if (err_traj) CK(cudaMemcpyAsync(hErr, h->traj_err, k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(hs, h->st, sizeof(StepState), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     if (energy_traj) memcpy(energy_traj + done, hE, k * sizeof(double));
     if (err_traj) memcpy(err_traj + done, hErr, k * sizeof(double));
-    if (hs->status) return status_error(h, hs->status);
+    const int status = *hstatus;
+    if (status < 0) return fail(SS_ERR_CUDA, "the step's status was not written");
+    if (status) return status_error(h, status);
   }
   return SS_OK;
 }

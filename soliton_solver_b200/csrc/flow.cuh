@@ -1081,9 +1081,11 @@ __global__ void __launch_bounds__(NT, (pipe_ctas<TH, MODE>())) flow_kernel_pipe(
   }
 }
 
-// Apply a pending arrest (V = 0) left by the trailing energy pass at the end of a call.
+// Apply a pending arrest (V = 0) left by the trailing energy pass at the end of a call,
+// and copy the call's status to status_out (nullable; e.g. mapped host memory).
 template <typename R>
-__global__ void finish_kernel(R* vel, long long n, const StepState* st) {
+__global__ void finish_kernel(R* vel, long long n, const StepState* st, int* status_out) {
+  if (status_out && blockIdx.x == 0 && threadIdx.x == 0) *(volatile int*)status_out = st->status;
   if (st->arrest == 0) return;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     vel[i] = (R)0;
