@@ -29,3 +29,24 @@ def test_reference_arm_prints_the_contract_line():
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_clock_summary_keeps_only_the_timed_region():
+    """bench.Clocks.summary(): the median SM clock, the max power and the union of the
+    clock-event reasons of the samples between the first and last mark()."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    c = bench.Clocks(0)
+    c.thread = object()  # as if the NVML poller had run
+    c.marks = [10.0, 10.02]
+    c.samples = [(9.99, 1000.0, 1965.0, 500.0, {"sw_power_cap"}),   # before the timed region
+                 (10.005, 1965.0, 1965.0, 270.0, set()),
+                 (10.010, 1950.0, 1965.0, 275.0, {"sw_power_cap"}),
+                 (10.015, 1965.0, 1965.0, 272.0, set()),
+                 (10.03, 900.0, 1965.0, 100.0, {"hw_slowdown"})]    # after it
+    s = c.summary()
+    assert s["samples"] == 3 and s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0
+    assert s["power_w_max"] == 275.0 and s["reasons"] == ["sw_power_cap"]
+    empty = bench.Clocks(0)
+    assert empty.summary()["sm_mhz"] is None
