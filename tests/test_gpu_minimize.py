@@ -1,8 +1,9 @@
 """Simulation.minimize: relaxation to max|dE/dphi| < tol through the product API (GPU).
 
 C2 (chiral magnet 320^2 over 10 x 10 J/D, Heusler, demag off, B = 0, anti-skyrmion, arrested
-Newton flow): the default FP32 schedule ("fp32+fp64": FP32 flow to its energy plateau,
-then FP64 on the projected state) must converge (err < 1e-6) without reaching max_steps,
+Newton flow): the default FP32 schedule ("fp32+fp64": FP32 flow until its energy plateaus
+or it stalls at FP32 resolution, then FP64 on the projected state) must converge (err < 1e-6)
+without reaching max_steps,
 and its relaxed energy must equal the FP64-only minimum to 1e-6 relative (the metric's
 accuracy gate; measured ~1e-11).  The FP32 phase's projected FP64 energy at the switch is
 within 1e-6 as well.
