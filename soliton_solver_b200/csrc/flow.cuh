@@ -446,6 +446,19 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, int 
         pre_l1[a] = gload<V, R>(A.la + a * N + sidx, FAST, v1);
       }
     }
+    // S4 one tile per CTA (FP32, up to four components): cP and cV likewise, where they are
+    // not staged
+    constexpr bool PRE4 = MODE == M_S4 && sizeof(R) == 4 && NF <= 4;
+    V pre_cp[PRE4 ? NF : 1], pre_cv[PRE4 ? NF : 1];
+    if constexpr (PRE4) {
+      if (!Cp) {
+#pragma unroll
+        for (int a = 0; a < NF; ++a) {
+          pre_cp[a] = gload<V, R>(A.cp + a * N + sidx, FAST, v1);
+          pre_cv[a] = gload<V, R>(A.cv + a * N + sidx, FAST, v1);
+        }
+      }
+    }
 
     Jet<V, NF> J;
     tile_jet<TH, V, R, TS::HY, TS::PLANE, FAST>(T, toff, kc, m0, m1, J);
@@ -547,8 +560,14 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, int 
 #pragma unroll
       for (int a = 0; a < NF; ++a) {
         const int coff = a * TX * TY + lx * TY + 2 * j;
-        const V cv = Cv ? ld_pair(Cv + coff) : gload<V, R>(A.cv + a * N + sidx, FAST, v1);
-        Pn[a] = Cp ? ld_pair(Cp + coff) : gload<V, R>(A.cp + a * N + sidx, FAST, v1);
+        V cv;
+        if constexpr (PRE4) {
+          cv = Cv ? ld_pair(Cv + coff) : pre_cv[a];
+          Pn[a] = Cp ? ld_pair(Cp + coff) : pre_cp[a];
+        } else {
+          cv = Cv ? ld_pair(Cv + coff) : gload<V, R>(A.cv + a * N + sidx, FAST, v1);
+          Pn[a] = Cp ? ld_pair(Cp + coff) : gload<V, R>(A.cp + a * N + sidx, FAST, v1);
+        }
         Vn[a] = vfma(sixth, mdt * g[a], cv);
         emax = fmax(emax, Lanes<V>::get(g[a], 0));
         if (v1) emax = fmax(emax, Lanes<V>::get(g[a], 1));
