@@ -854,14 +854,14 @@ __device__ __forceinline__ void flow_tile(const FlowArgs<R>& A, const CUtensorMa
 // of a tile is hidden only by other resident CTAs).  The fused FP32 stages 2+3 evaluate
 // two stencils per site pair: capped at three 256-thread CTAs (80 registers) for the
 // theories with up to four components and at two (128 registers; its 104 KB of staging
-// fits two anyway) for the six-component s+id.  FP64 stage 4 (one staged buffer) at two
-// 256-thread CTAs, 128 registers, up to four components (the s+id would spill ~380
-// bytes).  No bound otherwise.
+// fits two anyway) for the six-component s+id.  FP64 stages 1 and 4 and the energy pass
+// (one staged buffer each) at two 256-thread CTAs, 128 registers, up to four components
+// (the s+id would spill ~380 bytes).  No bound otherwise.
 template <class TH, typename R, int MODE, int NT>
 __host__ __device__ constexpr int flow_min_ctas() {
   if (NT != 256) return 1;
   if (sizeof(R) == 4 && MODE == M_S23) return TH::NF <= 4 ? 3 : 2;
-  if (sizeof(R) == 8 && MODE == M_S4) return TH::NF <= 4 ? 2 : 1;
+  if (sizeof(R) == 8 && (MODE == M_S4 || MODE == M_S1 || MODE == M_ENERGY)) return TH::NF <= 4 ? 2 : 1;
   return 1;
 }
 
