@@ -435,8 +435,8 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, int 
     const long long sidx = (long long)gx * G.Y + gy;
     // M_S23: the pair's V and l1 (overwritten by T2 and T3 in shared memory) come back
     // from L2; issued before the two stencils so that their latency hides behind them
-    // (up to four components: the six of the s+id model would spill)
-    constexpr bool PRE = MODE == M_S23 && NF <= 4;
+    // (FP32, up to four components: the six of the s+id model, and FP64 pairs, would spill)
+    constexpr bool PRE = MODE == M_S23 && NF <= 4 && sizeof(R) == 4;
     constexpr int NPRE = PRE ? NF : 1;
     V pre_v[NPRE], pre_l1[NPRE];
     if constexpr (PRE) {
