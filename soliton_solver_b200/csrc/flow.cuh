@@ -451,12 +451,10 @@ __device__ __forceinline__ void grad_tile(const FlowArgs<R>& A, const R* T, int 
     constexpr bool PRE4 = MODE == M_S4 && sizeof(R) == 4 && NF <= 4;
     V pre_cp[PRE4 ? NF : 1], pre_cv[PRE4 ? NF : 1];
     if constexpr (PRE4) {
-      if (!Cp) {
 #pragma unroll
-        for (int a = 0; a < NF; ++a) {
-          pre_cp[a] = gload<V, R>(A.cp + a * N + sidx, FAST, v1);
-          pre_cv[a] = gload<V, R>(A.cv + a * N + sidx, FAST, v1);
-        }
+      for (int a = 0; a < NF; ++a) {
+        if (!Cp) pre_cp[a] = gload<V, R>(A.cp + a * N + sidx, FAST, v1);
+        if (!Cv) pre_cv[a] = gload<V, R>(A.cv + a * N + sidx, FAST, v1);
       }
     }
 
