@@ -141,3 +141,29 @@ def test_field_densities(path):
     assert "supercurrent" in kinds and len(kinds) >= 2
     for k in kinds:
         _close(ref.field_density(th, F, p_i, p_f, k).reshape(-1), g[k])
+
+
+def test_relax_replay_with_the_oracles_own_decisions_is_relax():
+    """relax_replay (the oracle with given arrest decisions, used to check FP32 runs whose
+    decisions FP32 energies take) reproduces relax exactly when given relax's own
+    decisions: V = 0 after step s iff E[s] > E[s-1] (the first step compares with the
+    caller's previous energy, here +inf).  A run with arrests: Baby Skyrme from a field
+    with a large random velocity."""
+    from soliton_solver_b200.theories import load_theory
+
+    th = load_theory("Baby Skyrme")
+    rp = th.params.default_params(xlen=24, ylen=20, lsx=0.2, lsy=0.2, time_step=0.05,
+                                  unit_magnetization=True, killkinen=True).resolved()
+    p_i, p_f = th.params.pack_device_params(rp)
+    rng = np.random.default_rng(3)
+    F = rng.standard_normal((3, 24, 20))
+    F /= np.sqrt((F ** 2).sum(0))
+    V = 0.5 * rng.standard_normal(F.shape)
+    Fo, Vo, E, err = ref.relax("baby_skyrme", F, V, np.inf, p_i, p_f, 12)
+    arrests = np.concatenate([[False], np.diff(E) > 0])
+    assert arrests.any() and not arrests.all()
+    Fr, Vr, Er, errr = ref.relax_replay("baby_skyrme", F, V, arrests, p_i, p_f)
+    np.testing.assert_array_equal(Fr, Fo)
+    np.testing.assert_array_equal(Vr, Vo)
+    np.testing.assert_array_equal(Er, E)
+    np.testing.assert_array_equal(errr, err)
