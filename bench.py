@@ -321,8 +321,8 @@ def gpu_arm(args, rank, world, local_rank):
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     ms_step = ms / K
     value = world * N * K / (ms / 1e3) / 1e6
-    # stage launches per step, and the call's closing arrest kernel
-    launches = (3 if (s.tma_enabled and s._lib.ss_get_variant(s._h, 6) == 1) else 4) * K + 1
+    # stage launches per step, then the call's trailing energy pass and finish kernel
+    launches = (3 if (s.tma_enabled and s._lib.ss_get_variant(s._h, 6) == 1) else 4) * K + 2
 
     # roofline of the stage kernels (3 launches per step with stages 2 and 3 fused, else 4)
     from soliton_solver_b200._native import load as _load  # noqa: F401 (library loaded)
